@@ -1,0 +1,1324 @@
+// kernels.cu — sm_100a kernels and C ABI of the degree-4 nodal DG Euler hot
+// path (the operator of CFD-demo's src/cfd_demo/dg.py, limiting.py and
+// time_integration.py, driven by the run loop of solver.py).
+//
+// Design: one thread per element, element-major SoA state q[(c*15+j)*ld+e], so
+// every per-node load and store of a warp is one coalesced 256 B (double) or
+// 128 B (float) transaction. The 15x30 [Dr|Ds] contraction and the 15x15 LIFT
+// are compile-time constants (tables.cuh) applied as register-blocked FMAs:
+// each thread streams over the nodes j computing the contravariant fluxes
+// once and accumulating into a 15x4 register tile, then streams over its 15
+// face nodes (neighbour trace gathered from the neighbour's column, or a
+// boundary state), evaluates the interface flux and lifts the jump into the
+// same tile. The RK stage combine, the cell averages and — when the limiter
+// is `unlimited` — the positivity limiter, the stage minima and the CFL
+// reduction all happen in the same kernel, so one stage reads the state once
+// and writes it once. With slope limiting, a second light kernel per stage
+// (limit_kernel) reads the averages of the element and its neighbours plus
+// six midpoint traces and rewrites only troubled or non-positive elements.
+// Global reductions go through ordered 64-bit keys and one atomic per block.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "cfd_b200.h"
+#include "physics.cuh"
+#include "tables.cuh"
+
+namespace cfd {
+
+constexpr int NP = 15;
+constexpr int NFP = 5;
+constexpr double NEIGHBOR_FACTOR = 1.5;      // limiting.py:22
+constexpr double DETECTION_TOLERANCE = 1e-10; // limiting.py:24
+constexpr double POSITIVITY_FLOOR = 1e-13;    // limiting.py:28
+constexpr int BISECTION_STEPS = 60;           // limiting.py:29
+
+enum { MODE_RHS = 0, MODE_LIMITED = 1, MODE_UNLIMITED = 2 };
+// bits 0-1 decide admissibility; bit 2 marks a NaN CFL step (time_step -> NaN)
+enum { FLAG_NONFINITE = 1, FLAG_BAD_AVERAGE = 2, FLAG_NAN_DT = 4, FLAG_ADMISSIBILITY = 3 };
+
+// ---------------------------------------------------------------- helpers ---
+// Monotone map double -> uint64 so that unsigned integer order equals float order.
+__device__ __forceinline__ unsigned long long dkey(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__host__ __device__ __forceinline__ double dkey_decode(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  double d;
+  memcpy(&d, &b, sizeof(d));
+  return d;
+}
+constexpr unsigned long long KEY_EMPTY = ~0ull;
+
+__device__ __forceinline__ bool finite_(double x) { return isfinite(x); }
+__device__ __forceinline__ bool finite_(float x) { return isfinite(x); }
+
+// Face node k of face f, packed 4 bits per entry (tab::FACE_NODES_PACKED).
+constexpr unsigned long long FN_PACK = tab::FACE_NODES_PACKED;
+__device__ __forceinline__ int face_node_rt(int f, int k) { return (int)((FN_PACK >> (4 * (f * NFP + k))) & 15ull); }
+
+// FP32 form: drop the [Dr|Ds] entries that are round-off zeros of the
+// construction (|D| < 1e-13; 65 of 225 per matrix). The FP64 form keeps all.
+template <typename R> __host__ __device__ constexpr bool keep_entry(double v) {
+  return sizeof(R) == 8 ? true : (v > 1e-13 || v < -1e-13);
+}
+
+template <typename R> struct GeoPtr;
+template <> struct GeoPtr<double> {
+  static __device__ __forceinline__ const double* metric(const CfdMesh& m) { return m.metric; }
+  static __device__ __forceinline__ const double* face(const CfdMesh& m) { return m.face_geo; }
+  static __device__ __forceinline__ const double* cs(const CfdMesh& m) { return m.cs_coef; }
+};
+template <> struct GeoPtr<float> {
+  static __device__ __forceinline__ const float* metric(const CfdMesh& m) { return m.metric32; }
+  static __device__ __forceinline__ const float* face(const CfdMesh& m) { return m.face_geo32; }
+  static __device__ __forceinline__ const float* cs(const CfdMesh& m) { return m.cs_coef32; }
+};
+
+// Per-thread contribution to the per-instance stage reductions.
+struct Red {
+  double b[4];
+  unsigned long long kr, kp, kd;
+  int tr, fl;
+  __device__ void init() {
+    b[0] = b[1] = b[2] = b[3] = 0.0;
+    kr = kp = kd = KEY_EMPTY;
+    tr = 0;
+    fl = 0;
+  }
+};
+
+__device__ __forceinline__ void commit_one(const Red& r, CfdStageAcc* a) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (r.b[c] != 0.0) atomicAdd(&a->boundary_flux[c], r.b[c]);
+  if (r.kr != KEY_EMPTY) atomicMin(&a->min_rho_key, r.kr);
+  if (r.kp != KEY_EMPTY) atomicMin(&a->min_p_key, r.kp);
+  if (r.kd != KEY_EMPTY) atomicMin(&a->dt_key, r.kd);
+  if (r.tr) atomicAdd(&a->troubled, r.tr);
+  if (r.fl) atomicOr(&a->flags, r.fl);
+}
+
+// Reduce over the block and commit with one set of atomics when every live
+// thread belongs to the same instance (else each thread commits its own).
+// `slot(inst)` -> CfdStageAcc*. All threads of the block must call this.
+template <int BS>
+__device__ __forceinline__ void block_commit(Red r, bool live, int inst, CfdStageAcc* acc, int stride, int offset) {
+  __shared__ int s_inst;
+  __shared__ double s_b[BS / 32][4];
+  __shared__ unsigned long long s_k[BS / 32][3];
+  __shared__ int s_i[BS / 32][2];
+  if (threadIdx.x == 0) s_inst = live ? inst : -1;
+  __syncthreads();
+  const int inst0 = s_inst;
+  const bool uniform = __syncthreads_and(!live || inst == inst0) && inst0 >= 0;
+  if (!uniform) {
+    if (live) commit_one(r, acc + inst * stride + offset);
+    return;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) r.b[c] += __shfl_xor_sync(0xffffffffu, r.b[c], o);
+    r.kr = min(r.kr, __shfl_xor_sync(0xffffffffu, r.kr, o));
+    r.kp = min(r.kp, __shfl_xor_sync(0xffffffffu, r.kp, o));
+    r.kd = min(r.kd, __shfl_xor_sync(0xffffffffu, r.kd, o));
+    r.tr += __shfl_xor_sync(0xffffffffu, r.tr, o);
+    r.fl |= __shfl_xor_sync(0xffffffffu, r.fl, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) s_b[w][c] = r.b[c];
+    s_k[w][0] = r.kr;
+    s_k[w][1] = r.kp;
+    s_k[w][2] = r.kd;
+    s_i[w][0] = r.tr;
+    s_i[w][1] = r.fl;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Red t;
+    t.init();
+    for (int i = 0; i < BS / 32; ++i) {
+      for (int c = 0; c < 4; ++c) t.b[c] += s_b[i][c];
+      t.kr = min(t.kr, s_k[i][0]);
+      t.kp = min(t.kp, s_k[i][1]);
+      t.kd = min(t.kd, s_k[i][2]);
+      t.tr += s_i[i][0];
+      t.fl |= s_i[i][1];
+    }
+    commit_one(t, acc + inst0 * stride + offset);
+  }
+}
+
+// Pressure in double of a (possibly float) state: fast form (reciprocal,
+// contracted) and the reference's exact operation order (euler.py:21-27).
+__device__ __forceinline__ double pressure_d(double q0, double q1, double q2, double q3, double gm1) {
+  const double ir = __drcp_rn(q0);
+  return gm1 * (q3 - 0.5 * (q1 * (q1 * ir) + q2 * (q2 * ir)));
+}
+__device__ __forceinline__ double pressure_x(double q0, double q1, double q2, double q3, double gm1) {
+  return xmul(gm1, xsub(q3, xmul(0.5, xadd(xmul(q1, xdiv(q1, q0)), xmul(q2, xdiv(q2, q0))))));
+}
+// The fast form, replaced by the exact one wherever the two could fall on
+// different sides of `bound` (they differ by a few ulps of |E| + |m.u|).
+__device__ __forceinline__ double pressure_near(double q0, double q1, double q2, double q3, double gm1, double bound) {
+  const double ir = __drcp_rn(q0);
+  const double k = 0.5 * (q1 * (q1 * ir) + q2 * (q2 * ir));
+  const double p = gm1 * (q3 - k);
+  const double margin = 1e-13 * (fabs(q3) + fabs(k)) + 1e-300;
+  return (p - bound > margin || p != p) ? p : pressure_x(q0, q1, q2, q3, gm1);
+}
+
+// Cell average in double, sequential and unfused like NumPy's einsum
+// (limiting.py:209, dg.py:168-171).
+template <typename R>
+__device__ __forceinline__ void cell_average(const R (&q)[NP][4], double a[4]) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    double s = xmul(tab::AVG_W[0], (double)q[0][c]);
+#pragma unroll
+    for (int i = 1; i < NP; ++i) s = xadd(s, xmul(tab::AVG_W[i], (double)q[i][c]));
+    a[c] = s;
+  }
+}
+
+// Zhang-Shu positivity scaling of one element toward its average, in double
+// and in the reference's operation order (limiting.py:166-200). q is the
+// element's nodal state in registers. Returns true if q changed.
+template <typename R>
+__device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], double gm1) {
+  const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
+  const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+  double rmin = (double)q[0][0];
+#pragma unroll
+  for (int i = 1; i < NP; ++i) rmin = jmin(rmin, (double)q[i][0]);
+  bool changed = false;
+  if (rmin < eps) {
+    const double span = xsub(a[0], rmin);
+    const double theta = jmin(jmax(xdiv(xsub(a[0], eps), span), 0.0), 1.0);
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) q[i][c] = (R)xadd(a[c], xmul(theta, xsub((double)q[i][c], a[c])));
+    changed = true;
+  }
+  unsigned need = 0;
+#pragma unroll
+  for (int i = 0; i < NP; ++i)
+    if (pressure_near(q[i][0], q[i][1], q[i][2], q[i][3], gm1, eps) < eps) need |= 1u << i;
+  if (!need) return changed;
+  double theta = 1.0;
+#pragma unroll 1
+  for (int i = 0; i < NP; ++i) {
+    if (!((need >> i) & 1u)) continue;
+    double qi[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      // select node i without dynamic register indexing
+      double v = 0.0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) v = (j == i) ? (double)q[j][c] : v;
+      qi[c] = v;
+    }
+    const double d0 = xsub(qi[0], a[0]), d1 = xsub(qi[1], a[1]), d2 = xsub(qi[2], a[2]), d3 = xsub(qi[3], a[3]);
+    double lo = 0.0, hi = 1.0;
+#pragma unroll 1
+    for (int it = 0; it < BISECTION_STEPS; ++it) {
+      const double mid = xmul(0.5, xadd(lo, hi));
+      const bool ok = pressure_x(xadd(a[0], xmul(mid, d0)), xadd(a[1], xmul(mid, d1)), xadd(a[2], xmul(mid, d2)),
+                                 xadd(a[3], xmul(mid, d3)), gm1) >= eps;
+      lo = ok ? mid : lo;
+      hi = ok ? hi : mid;
+    }
+    theta = jmin(theta, lo);
+  }
+  if (theta < 1.0) {
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) q[i][c] = (R)xadd(a[c], xmul(theta, xsub((double)q[i][c], a[c])));
+    changed = true;
+  }
+  return changed;
+}
+
+// Nodal minima (density, pressure; NaN ignored), max wave speed and finiteness.
+template <typename R>
+__device__ __forceinline__ void element_stats(const R (&q)[NP][4], double gm1, double gamma, double& rmin, double& pmin,
+                                              double& lam, bool& finite) {
+  rmin = INFINITY;
+  pmin = INFINITY;
+  lam = -INFINITY;
+  finite = true;
+  bool lam_nan = false;
+#pragma unroll
+  for (int i = 0; i < NP; ++i) {
+    const double r = q[i][0], mx = q[i][1], my = q[i][2], en = q[i][3];
+    const double ir = __drcp_rn(r);
+    const double u = mx * ir, v = my * ir;
+    const double p = pressure_near(r, mx, my, en, gm1, 0.0);
+    rmin = fmin(rmin, r);
+    pmin = fmin(pmin, p);
+    // time_integration.py:39-40: |u| + c
+    const double s = sqrt(u * u + v * v) + sqrt(gamma * p * ir);
+    lam_nan |= (s != s);
+    lam = fmax(lam, s);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) finite &= finite_(q[i][c]);
+  }
+  if (lam_nan) lam = NAN;
+}
+
+
+// ---- volume term: acc = -(Dr Ft + Ds Gt), Ft = rx F + ry G, Gt = sx F + sy G
+// (dg.py:148-151). Fully unrolled: [Dr|Ds] are immediates / constant-bank
+// operands and round-off zeros are skipped at compile time (FP32 form).
+template <typename R>
+__device__ __forceinline__ void volume_unrolled(const R* __restrict__ src, int e, int ld, R gm1, R rx, R ry, R sx, R sy,
+                                                R (&acc)[NP][4]) {
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    R qj[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qj[c] = src[(c * NP + j) * ld + e];
+    const Prim<R> w = primitive(qj, gm1);
+    R f[4], g[4];
+    cartesian(qj, w, f, g);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const R ft = rx * f[c] + ry * g[c];
+      const R gt = sx * f[c] + sy * g[c];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        R t = (j == 0) ? R(0) : acc[i][c];
+        if (keep_entry<R>(tab::DR[i][j])) t = fma((R)(-tab::DR[i][j]), ft, t);
+        if (keep_entry<R>(tab::DS[i][j])) t = fma((R)(-tab::DS[i][j]), gt, t);
+        acc[i][c] = t;
+      }
+    }
+  }
+}
+
+// Rolled over j (FP64 form): the 120-register accumulator tile stays resident
+// and the table column is a warp-uniform constant-bank read.
+template <typename R>
+__device__ __forceinline__ void volume_rolled(const R* __restrict__ src, int e, int ld, R gm1, R rx, R ry, R sx, R sy,
+                                              R (&acc)[NP][4]) {
+#pragma unroll
+  for (int i = 0; i < NP; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[i][c] = R(0);
+#pragma unroll 1
+  for (int j = 0; j < NP; ++j) {
+    R qj[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qj[c] = src[(c * NP + j) * ld + e];
+    const Prim<R> w = primitive(qj, gm1);
+    R f[4], g[4];
+    cartesian(qj, w, f, g);
+    R ft[4], gt[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      ft[c] = rx * f[c] + ry * g[c];
+      gt[c] = sx * f[c] + sy * g[c];
+    }
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      const R dr = (R)ctab::DR[i][j], ds = (R)ctab::DS[i][j];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[i][c] = fma(-ds, gt[c], fma(-dr, ft[c], acc[i][c]));
+    }
+  }
+}
+
+// One face node of the surface term: exterior state, interface flux, lifted
+// jump, boundary-flux contribution (dg.py:153-164, boundary: dg.py:119-137).
+template <typename R, int FLUX>
+__device__ __forceinline__ void face_node_flux(const CfdMesh& m, const R* __restrict__ src, int e, int ld, R gamma,
+                                               int n, int kind, int nb, int pn, R nx, R ny, R fs, double bw,
+                                               R jump[4], Red& red) {
+  R qm[4], qp[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) qm[c] = src[(c * NP + n) * ld + e];
+  if (kind == CFD_FACE_INTERIOR) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qp[c] = src[(c * NP + pn) * ld + nb];
+  } else if (kind == CFD_FACE_SLIP_WALL) {
+    const R mn = qm[1] * nx + qm[2] * ny;
+    qp[0] = qm[0];
+    qp[1] = qm[1] - R(2) * mn * nx;
+    qp[2] = qm[2] - R(2) * mn * ny;
+    qp[3] = qm[3];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[nb * 4 + c];
+  }
+  R fhat[4], fm[4];
+  interface_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) jump[c] = fs * (fm[c] - fhat[c]);
+  if (kind != CFD_FACE_INTERIOR) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) red.b[c] += bw * (double)fhat[c];
+  }
+}
+
+template <typename R, int FLUX>
+__device__ __forceinline__ void surface_unrolled(const CfdMesh& m, const R* __restrict__ src, int e, int ld, R gamma,
+                                                 R (&acc)[NP][4], Red& red) {
+  const R* __restrict__ fg = GeoPtr<R>::face(m);
+  const int finfo = m.face_info[e];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const int info = (finfo >> (8 * f)) & 0xff;
+    const int kind = info & 3;
+    const int nf = (info >> 2) & 3;
+    const R nx = fg[(3 * f) * ld + e], ny = fg[(3 * f + 1) * ld + e], fs = fg[(3 * f + 2) * ld + e];
+    const int nb = (kind != CFD_FACE_SLIP_WALL) ? m.neighbor[f * ld + e] : 0;
+    const double hl = (kind != CFD_FACE_INTERIOR) ? m.face_hlen[f * ld + e] : 0.0;
+    const bool same_order = (f == 2) != (nf == 2);
+#pragma unroll
+    for (int k = 0; k < NFP; ++k) {
+      const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);
+      R jump[4];
+      face_node_flux<R, FLUX>(m, src, e, ld, gamma, tab::FACE_NODES[f][k], kind, nb, pn, nx, ny, fs,
+                              tab::FACE_W[k] * hl, jump, red);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int i = 0; i < NP; ++i) acc[i][c] = fma((R)tab::LIFT[i][f * NFP + k], jump[c], acc[i][c]);
+    }
+  }
+}
+
+template <typename R, int FLUX>
+__device__ __forceinline__ void surface_rolled(const CfdMesh& m, const R* __restrict__ src, int e, int ld, R gamma,
+                                               R (&acc)[NP][4], Red& red) {
+  const R* __restrict__ fg = GeoPtr<R>::face(m);
+  const int finfo = m.face_info[e];
+#pragma unroll 1
+  for (int f = 0; f < 3; ++f) {
+    const int info = (finfo >> (8 * f)) & 0xff;
+    const int kind = info & 3;
+    const int nf = (info >> 2) & 3;
+    const R nx = fg[(3 * f) * ld + e], ny = fg[(3 * f + 1) * ld + e], fs = fg[(3 * f + 2) * ld + e];
+    const int nb = (kind != CFD_FACE_SLIP_WALL) ? m.neighbor[f * ld + e] : 0;
+    const double hl = (kind != CFD_FACE_INTERIOR) ? m.face_hlen[f * ld + e] : 0.0;
+    const bool same_order = (f == 2) != (nf == 2);
+#pragma unroll 1
+    for (int k = 0; k < NFP; ++k) {
+      const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);
+      R jump[4];
+      face_node_flux<R, FLUX>(m, src, e, ld, gamma, ctab::FACE_NODES[f][k], kind, nb, pn, nx, ny, fs,
+                              ctab::FACE_W[k] * hl, jump, red);
+      const int col = f * NFP + k;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const R l = (R)ctab::LIFT[i][col];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[i][c] = fma(l, jump[c], acc[i][c]);
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------- stage kernel ---
+struct StageParams {
+  CfdMesh m;
+  const CfdControl* ctl;
+  const void* x0;
+  const void* x1;
+  void* stage;
+  int stage_idx;  // 1..3; 0 = rhs only
+  double gamma;
+  double* avg;
+  double* aux;
+  CfdStageAcc* acc;
+  const void* q_in;  // MODE_RHS
+  void* q_out;       // MODE_RHS
+  double* bflux_out; // MODE_RHS, [instances][4]
+};
+
+template <typename R>
+__device__ __forceinline__ void select_buffers(const StageParams& P, int par, const R*& src, const R*& base, R*& dst) {
+  const R* cur = (const R*)(par ? P.x1 : P.x0);
+  R* nxt = (R*)(par ? P.x0 : P.x1);
+  if (P.stage_idx == 1) {
+    src = cur;
+    base = nullptr;
+    dst = nxt;
+  } else if (P.stage_idx == 2) {
+    src = nxt;
+    base = cur;
+    dst = (R*)P.stage;
+  } else {
+    src = (const R*)P.stage;
+    base = cur;
+    dst = nxt;
+  }
+}
+
+template <typename R, int FLUX, int MODE, int BS>
+__global__ void __launch_bounds__(BS) stage_kernel(const StageParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * BS + threadIdx.x;
+  bool live = e < m.num_elements;
+  int inst = 0;
+  if (live && m.instance) inst = m.instance[e];
+  double dt = 0.0;
+  int par = 0;
+  if (live && MODE != MODE_RHS) {
+    const CfdControl* c = P.ctl + inst;
+    live = c->status == CFD_RUN_ACTIVE;
+    dt = c->dt;
+    par = c->parity;
+  }
+  Red red;
+  red.init();
+  if (live) {
+    const R* src_;
+    const R* base_;
+    R* dst_;
+    if (MODE == MODE_RHS) {
+      src_ = (const R*)P.q_in;
+      base_ = nullptr;
+      dst_ = (R*)P.q_out;
+    } else {
+      select_buffers<R>(P, par, src_, base_, dst_);
+    }
+    const R* __restrict__ src = src_;
+    const R* __restrict__ base = base_;
+    R* __restrict__ dst = dst_;
+    const R gamma = (R)P.gamma;
+    const R gm1 = gamma - R(1);
+    const R* __restrict__ mg = GeoPtr<R>::metric(m);
+    const R rx = mg[e], ry = mg[ld + e], sx = mg[2 * ld + e], sy = mg[3 * ld + e];
+
+    R acc[NP][4];
+    if (sizeof(R) == 4) {
+      volume_unrolled<R>(src, e, ld, gm1, rx, ry, sx, sy, acc);
+      surface_unrolled<R, FLUX>(m, src, e, ld, gamma, acc, red);
+    } else {
+      volume_rolled<R>(src, e, ld, gm1, rx, ry, sx, sy, acc);
+      surface_rolled<R, FLUX>(m, src, e, ld, gamma, acc, red);
+    }
+
+    if (MODE == MODE_RHS) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dst[(c * NP + i) * ld + e] = acc[i][c];
+    } else {
+      // ---- SSP-RK3 stage combine (time_integration.py:61-66)
+      const R rdt = (R)dt;
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int idx = (c * NP + i) * ld + e;
+          const R v = src[idx] + rdt * acc[i][c];
+          if (P.stage_idx == 1) acc[i][c] = v;
+          else if (P.stage_idx == 2) acc[i][c] = R(0.75) * base[idx] + R(0.25) * v;
+          else acc[i][c] = base[idx] * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
+        }
+      // ---- cell averages in double (limiting.py:209)
+      double a[4];
+      cell_average<R>(acc, a);
+      const double gm1d = P.gamma - 1.0;
+      const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1d);
+      if (!(a[0] > 0.0) || !(pa > 0.0)) red.fl |= FLAG_BAD_AVERAGE;
+      if (MODE == MODE_UNLIMITED) positivity<R>(acc, a, gm1d);
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dst[(c * NP + i) * ld + e] = acc[i][c];
+      double rmin, pmin, lam;
+      bool finite;
+      element_stats<R>(acc, gm1d, P.gamma, rmin, pmin, lam, finite);
+      if (!finite) red.fl |= FLAG_NONFINITE;
+      if (MODE == MODE_LIMITED) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) P.avg[c * ld + e] = a[c];
+        P.aux[e] = rmin;
+        P.aux[ld + e] = pmin;
+        if (P.stage_idx == 3) P.aux[2 * ld + e] = lam;
+      } else {
+        red.kr = dkey(rmin);
+        red.kp = dkey(pmin);
+        if (P.stage_idx == 3) {
+          const double d = m.dt_geo[e] / lam;
+          red.kd = dkey(d);
+          if (d != d) red.fl |= FLAG_NAN_DT;
+        }
+      }
+    }
+  }
+  if (MODE == MODE_RHS) {
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (red.b[c] != 0.0) atomicAdd(&P.bflux_out[inst * 4 + c], red.b[c]);
+    }
+  } else {
+    block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
+  }
+}
+
+// ----------------------------------------------------------- limit kernel ---
+struct LimitParams {
+  CfdMesh m;
+  const CfdControl* ctl;  // null: always active (cfd_limit)
+  const void* x0;
+  const void* x1;
+  void* stage;
+  int stage_idx;          // 1..3, or 0 with q = q_io (cfd_limit)
+  void* q_io;
+  double gamma;
+  const double* avg;
+  const double* aux;
+  CfdStageAcc* acc;       // stage mode
+  int32_t* troubled_out;  // cfd_limit mode
+};
+
+// Cockburn-Shu troubled-cell limiter (limiting.py:136-163) followed by the
+// positivity limiter (limiting.py:166-200), in place on the stage state.
+template <typename R, int PHI, int BS>
+__global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * BS + threadIdx.x;
+  bool live = e < m.num_elements;
+  int inst = 0;
+  if (live && m.instance) inst = m.instance[e];
+  int par = 0;
+  if (live && P.ctl) {
+    live = P.ctl[inst].status == CFD_RUN_ACTIVE;
+    par = P.ctl[inst].parity;
+  }
+  Red red;
+  red.init();
+  if (live) {
+    R* __restrict__ q;
+    if (P.stage_idx == 0) {
+      q = (R*)P.q_io;
+    } else if (P.stage_idx == 2) {
+      q = (R*)P.stage;
+    } else {
+      q = (R*)(par ? P.x0 : P.x1);
+    }
+    const double gm1 = P.gamma - 1.0;
+    double a[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) a[c] = P.avg[c * ld + e];
+    const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
+    const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+    const int finfo = m.face_info[e];
+    bool troubled = false;
+    R scaled[3][4];
+    if (PHI != LIM_UNLIMITED) {
+      // neighbour / ghost averages (limiting.py:128-133), unfused as in NumPy
+      R diff[3][4];
+      const double* fgd = m.face_geo;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        const int kind = (finfo >> (8 * f)) & 3;
+        double na[4];
+        if (kind == CFD_FACE_INTERIOR) {
+          const int nb = m.neighbor[f * ld + e];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) na[c] = P.avg[c * ld + nb];
+        } else if (kind == CFD_FACE_SLIP_WALL) {
+          const double nx = fgd[(3 * f) * ld + e], ny = fgd[(3 * f + 1) * ld + e];
+          const double mn = xadd(xmul(a[1], nx), xmul(a[2], ny));
+          na[0] = a[0];
+          na[1] = xsub(a[1], xmul(xmul(2.0, mn), nx));
+          na[2] = xsub(a[2], xmul(xmul(2.0, mn), ny));
+          na[3] = a[3];
+        } else {
+          const int row = m.neighbor[f * ld + e];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) na[c] = m.bc_states[row * 4 + c];
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) diff[f][c] = (R)xsub(na[c], a[c]);
+      }
+      const R* __restrict__ cs = GeoPtr<R>::cs(m);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        const int pf = (finfo >> (8 * f + 4)) & 3;
+        const R al = cs[f * ld + e], be = cs[(3 + f) * ld + e];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const R pd = pf == 0 ? diff[0][c] : (pf == 1 ? diff[1][c] : diff[2][c]);
+          scaled[f][c] = xmul((R)NEIGHBOR_FACTOR, xadd(xmul(al, diff[f][c]), xmul(be, pd)));
+        }
+      }
+      // detection on rho and E at the three face midpoints (limiting.py:147-151)
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int c = cc == 0 ? 0 : 3;
+          const R tr = xsub(q[(c * NP + tab::MID_NODES[f]) * ld + e], (R)a[c]);
+          const R ex = abs_(xsub(minmod2(tr, scaled[f][c]), tr));
+          troubled |= (double)ex > xmul(DETECTION_TOLERANCE, fabs(a[c]));
+        }
+      }
+    }
+    const double rmin0 = P.aux[e], pmin0 = P.aux[ld + e];
+    const bool need_pos = (rmin0 < eps) || (pmin0 < eps);
+    if (!troubled && !need_pos) {
+      red.kr = dkey(rmin0);
+      red.kp = dkey(pmin0);
+      if (P.stage_idx == 3) {
+        const double d = m.dt_geo[e] / P.aux[2 * ld + e];
+        red.kd = dkey(d);
+        if (d != d) red.fl |= FLAG_NAN_DT;
+      }
+    } else {
+      R s[NP][4];
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s[i][c] = q[(c * NP + i) * ld + e];
+      if (troubled) {
+        // P1 midpoint values, phi-limited deltas, +/- rescaling, linear rebuild
+        // (limiting.py:153-162), in NumPy's operation order
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const R ac = (R)a[c];
+          R deltas[3];
+          R pos = R(0), neg = R(0);
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            R pr = xmul((R)tab::P1MID[f][0], s[0][c]);
+#pragma unroll
+            for (int i = 1; i < NP; ++i) pr = xadd(pr, xmul((R)tab::P1MID[f][i], s[i][c]));
+            pr = xsub(pr, ac);
+            R d = R(0);
+            if (pr != R(0)) d = xmul(pr, jmin(R(1), phi<R, PHI>(xdiv(scaled[f][c], pr))));
+            deltas[f] = d;
+            pos = f == 0 ? jmax(d, R(0)) : xadd(pos, jmax(d, R(0)));
+            neg = f == 0 ? jmax(-d, R(0)) : xadd(neg, jmax(-d, R(0)));
+          }
+          const R thp = pos > R(0) ? jmin(R(1), xdiv(neg, pos)) : R(0);
+          const R thn = neg > R(0) ? jmin(R(1), xdiv(pos, neg)) : R(0);
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            deltas[f] = xsub(xmul(thp, jmax(deltas[f], R(0))), xmul(thn, jmax(-deltas[f], R(0))));
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            R v = xmul((R)tab::LINBASIS[i][0], deltas[0]);
+            v = xadd(v, xmul((R)tab::LINBASIS[i][1], deltas[1]));
+            v = xadd(v, xmul((R)tab::LINBASIS[i][2], deltas[2]));
+            s[i][c] = xadd(ac, v);
+          }
+        }
+        red.tr = 1;
+      }
+      positivity<R>(s, a, gm1);
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) q[(c * NP + i) * ld + e] = s[i][c];
+      double rmin, pmin, lam;
+      bool finite;
+      element_stats<R>(s, gm1, P.gamma, rmin, pmin, lam, finite);
+      if (!finite) red.fl |= FLAG_NONFINITE;
+      red.kr = dkey(rmin);
+      red.kp = dkey(pmin);
+      if (P.stage_idx == 3) {
+        const double d = m.dt_geo[e] / lam;
+        red.kd = dkey(d);
+        if (d != d) red.fl |= FLAG_NAN_DT;
+      }
+    }
+  }
+  if (P.stage_idx == 0) {
+    if (live && red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
+  } else {
+    block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
+  }
+}
+
+// Averages + per-element minima of q_in, copied to q_out (cfd_limit prologue).
+template <typename R, int BS>
+__global__ void __launch_bounds__(BS) prep_kernel(CfdMesh m, const R* __restrict__ qin, R* __restrict__ qout,
+                                                   double* avg, double* aux, double gamma) {
+  const int e = blockIdx.x * BS + threadIdx.x;
+  if (e >= m.num_elements) return;
+  const int ld = m.ld;
+  R s[NP][4];
+#pragma unroll
+  for (int i = 0; i < NP; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      s[i][c] = qin[(c * NP + i) * ld + e];
+      if (qout != qin) qout[(c * NP + i) * ld + e] = s[i][c];
+    }
+  double a[4];
+  cell_average<R>(s, a);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) avg[c * ld + e] = a[c];
+  double rmin, pmin, lam;
+  bool finite;
+  element_stats<R>(s, gamma - 1.0, gamma, rmin, pmin, lam, finite);
+  aux[e] = rmin;
+  aux[ld + e] = pmin;
+  aux[2 * ld + e] = lam;
+}
+
+// ---------------------------------------------------------- small kernels ---
+template <typename R, int BS>
+__global__ void __launch_bounds__(BS) dt_kernel(CfdMesh m, const R* __restrict__ q, CfdStageAcc* acc, double gamma,
+                                                 double* minima) {
+  const int e = blockIdx.x * BS + threadIdx.x;
+  const bool live = e < m.num_elements;
+  const int inst = (live && m.instance) ? m.instance[e] : 0;
+  Red red;
+  red.init();
+  if (live) {
+    const int ld = m.ld;
+    R s[NP][4];
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s[i][c] = q[(c * NP + i) * ld + e];
+    double rmin, pmin, lam;
+    bool finite;
+    element_stats<R>(s, gamma - 1.0, gamma, rmin, pmin, lam, finite);
+    // time_integration.py:41 — the min propagates NaN: a NaN element poisons dt
+    const double d = m.dt_geo[e] / lam;
+    red.kd = dkey(d);
+    if (d != d) red.fl |= FLAG_NAN_DT;
+    red.kr = dkey(rmin);
+    red.kp = dkey(pmin);
+    if (!finite) red.fl |= FLAG_NONFINITE;
+  }
+  block_commit<BS>(red, live, inst, acc, 3, 2);
+}
+
+__global__ void reset_acc_kernel(CfdStageAcc* acc, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  CfdStageAcc z;
+  z.boundary_flux[0] = z.boundary_flux[1] = z.boundary_flux[2] = z.boundary_flux[3] = 0.0;
+  z.min_rho_key = z.min_p_key = z.dt_key = KEY_EMPTY;
+  z.troubled = 0;
+  z.flags = 0;
+  acc[i] = z;
+}
+
+__device__ __forceinline__ double key_min_value(unsigned long long k) {
+  return k == KEY_EMPTY ? INFINITY : dkey_decode(k);
+}
+
+// StepReport of one attempt (time_integration.py:69-83).
+__global__ void report_kernel(const CfdStageAcc* acc, const CfdControl* ctl, CfdStepReport* rep, int n, double cfl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (ctl[i].status != CFD_RUN_ACTIVE) return;
+  const CfdStageAcc* a = acc + 3 * i;
+  const double dt = ctl[i].dt;
+  CfdStepReport r;
+  for (int c = 0; c < 4; ++c)
+    r.boundary_flux[c] = dt * (a[0].boundary_flux[c] / 6.0 + a[1].boundary_flux[c] / 6.0 + 2.0 * a[2].boundary_flux[c] / 3.0);
+  const int fl = a[0].flags | a[1].flags | a[2].flags;
+  r.admissible = (fl & FLAG_ADMISSIBILITY) == 0;
+  double rmin = INFINITY, pmin = INFINITY;
+  int tr = 0;
+  for (int s = 0; s < 3; ++s) {
+    rmin = fmin(rmin, key_min_value(a[s].min_rho_key));
+    pmin = fmin(pmin, key_min_value(a[s].min_p_key));
+    tr = max(tr, a[s].troubled);
+  }
+  if (fl & FLAG_NONFINITE) {
+    rmin = NAN;
+    pmin = NAN;
+  }
+  r.min_density = rmin;
+  r.min_pressure = pmin;
+  r.troubled_cells = tr;
+  r.dt = dt;
+  r.dt_next = (a[2].flags & FLAG_NAN_DT) ? (double)NAN : cfl * dkey_decode(a[2].dt_key);
+  r.reserved[0] = r.reserved[1] = 0;
+  rep[i] = r;
+}
+
+// One pass of the body of solver.py:180-204 after an attempt.
+__global__ void run_control_kernel(CfdControl* ctl, const CfdStepReport* rep, int n, int max_rejections) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  CfdControl c = ctl[i];
+  if (c.status != CFD_RUN_ACTIVE) return;
+  const CfdStepReport r = rep[i];
+  if (r.admissible) {
+    c.parity ^= 1;
+    c.time = c.reaches_end ? c.final_time : c.time + c.dt;
+    c.steps += 1;
+    for (int k = 0; k < 4; ++k) c.flux_integral[k] += r.boundary_flux[k];
+    if (r.min_density < c.min_density) c.min_density = r.min_density;
+    if (r.min_pressure < c.min_pressure) c.min_pressure = r.min_pressure;
+    c.max_troubled = max(c.max_troubled, r.troubled_cells);
+    c.attempts = 0;
+    if (!(c.time < c.final_time)) {
+      c.status = CFD_RUN_DONE;
+    } else {
+      const double dt = r.dt_next;
+      if (!isfinite(dt) || dt <= 0.0) {
+        c.status = CFD_RUN_BAD_DT;
+        c.dt = dt;
+      } else {
+        const double remaining = c.final_time - c.time;
+        c.reaches_end = dt >= remaining;
+        c.dt = c.reaches_end ? remaining : dt;
+      }
+    }
+  } else {
+    c.rejected += 1;
+    c.attempts += 1;
+    if (c.attempts >= max_rejections + 1) {
+      c.status = CFD_RUN_REJECTED;
+    } else {
+      c.reaches_end = 0;
+      c.dt *= 0.5;
+    }
+  }
+  ctl[i] = c;
+}
+
+__global__ void run_init_kernel(CfdControl* ctl, const CfdStageAcc* acc, const double* final_time, int n, double cfl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  CfdControl c;
+  memset(&c, 0, sizeof(c));
+  c.final_time = final_time[i];
+  const CfdStageAcc a = acc[3 * i + 2];
+  c.min_density = key_min_value(a.min_rho_key);
+  c.min_pressure = key_min_value(a.min_p_key);
+  c.status = CFD_RUN_ACTIVE;
+  if (!(c.time < c.final_time)) {
+    c.status = CFD_RUN_DONE;
+  } else {
+    const double dt = (a.flags & FLAG_NAN_DT) ? (double)NAN : cfl * dkey_decode(a.dt_key);
+    if (!isfinite(dt) || dt <= 0.0) {
+      c.status = CFD_RUN_BAD_DT;
+      c.dt = dt;
+    } else {
+      const double remaining = c.final_time - c.time;
+      c.reaches_end = dt >= remaining;
+      c.dt = c.reaches_end ? remaining : dt;
+    }
+  }
+  ctl[i] = c;
+}
+
+__global__ void dt_out_kernel(const CfdStageAcc* acc, double* dt, int n, double cfl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dt[i] = (acc[3 * i + 2].flags & FLAG_NAN_DT) ? (double)NAN : cfl * dkey_decode(acc[3 * i + 2].dt_key);
+}
+
+__global__ void check_out_kernel(const CfdStageAcc* acc, double* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const CfdStageAcc a = acc[3 * i + 2];
+  out[3 * i + 0] = key_min_value(a.min_rho_key);
+  out[3 * i + 1] = key_min_value(a.min_p_key);
+  out[3 * i + 2] = (a.flags & FLAG_NONFINITE) ? 0.0 : 1.0;
+}
+
+// (Np, K, 4) double  <->  [(c*15+j)*ld + e] of R
+template <typename R>
+__global__ void pack_kernel(const double* __restrict__ in, R* __restrict__ out, int K, int ld) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)NP * K) return;
+  const int j = (int)(t / K), e = (int)(t % K);
+  const double4 v = reinterpret_cast<const double4*>(in)[t];
+  out[(0 * NP + j) * (long long)ld + e] = (R)v.x;
+  out[(1 * NP + j) * (long long)ld + e] = (R)v.y;
+  out[(2 * NP + j) * (long long)ld + e] = (R)v.z;
+  out[(3 * NP + j) * (long long)ld + e] = (R)v.w;
+}
+template <typename R>
+__global__ void unpack_kernel(const R* __restrict__ in, double* __restrict__ out, int K, int ld) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)NP * K) return;
+  const int j = (int)(t / K), e = (int)(t % K);
+  double4 v;
+  v.x = (double)in[(0 * NP + j) * (long long)ld + e];
+  v.y = (double)in[(1 * NP + j) * (long long)ld + e];
+  v.z = (double)in[(2 * NP + j) * (long long)ld + e];
+  v.w = (double)in[(3 * NP + j) * (long long)ld + e];
+  reinterpret_cast<double4*>(out)[t] = v;
+}
+
+template <typename R>
+__global__ void averages_kernel(CfdMesh m, const R* __restrict__ q, double* avg, double* integral) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.num_elements) return;
+  const int ld = m.ld;
+  const int inst = m.instance ? m.instance[e] : 0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) s = fma(avg ? tab::AVG_W[i] : tab::CELL_W[i], (double)q[(c * NP + i) * ld + e], s);
+    if (avg) avg[c * ld + e] = s;
+    else atomicAdd(&integral[inst * 4 + c], m.jacobian[e] * s);  // dg.py:174-176
+  }
+}
+
+template <int FLUX>
+__global__ void flux_pointwise_kernel(int n, const double* qm, const double* qp, const double* nx, const double* ny,
+                                      double gamma, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a[4], b[4], fh[4], fm[4];
+  for (int c = 0; c < 4; ++c) {
+    a[c] = qm[4 * i + c];
+    b[c] = qp[4 * i + c];
+  }
+  interface_flux<double, FLUX>(a, b, nx[i], ny[i], gamma, fh, fm);
+  for (int c = 0; c < 4; ++c) out[4 * i + c] = fh[c];
+}
+
+template <int PHI>
+__global__ void phi_pointwise_kernel(int n, const double* r, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = phi<double, PHI>(r[i]);
+}
+
+}  // namespace cfd
+
+// ================================================================= C ABI ===
+using namespace cfd;
+
+static thread_local char g_err[512] = "";
+
+static int fail(int code, const char* msg) {
+  snprintf(g_err, sizeof(g_err), "%s", msg);
+  return code;
+}
+static int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+    return CFD_E_CUDA;
+  }
+  return CFD_OK;
+}
+
+static int validate(const CfdSolver* s) {
+  if (!s) return fail(CFD_E_ARG, "null solver");
+  const CfdMesh& m = s->mesh;
+  if (m.num_elements <= 0 || m.ld < m.num_elements || m.num_instances < 1) return fail(CFD_E_ARG, "bad mesh sizes");
+  if (!m.metric || !m.face_geo || !m.face_hlen || !m.dt_geo || !m.jacobian || !m.cs_coef || !m.neighbor || !m.face_info)
+    return fail(CFD_E_ARG, "mesh table pointer is null");
+  if (m.num_instances > 1 && !m.instance) return fail(CFD_E_ARG, "instance table needed for several instances");
+  if (s->flux < 0 || s->flux > 2) return fail(CFD_E_ARG, "unknown flux id");
+  if (s->limiter < 0 || s->limiter > 4) return fail(CFD_E_ARG, "unknown limiter id");
+  if (s->precision != CFD_FP64 && s->precision != CFD_FP32_MIXED) return fail(CFD_E_ARG, "unknown precision id");
+  if (s->precision == CFD_FP32_MIXED && (!m.metric32 || !m.face_geo32 || !m.cs_coef32))
+    return fail(CFD_E_ARG, "FP32 mesh tables missing for the mixed precision");
+  if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
+  if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
+    return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
+  return CFD_OK;
+}
+
+static inline int bs_of(const CfdSolver* s) { return s->block_size ? s->block_size : 128; }
+static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// Dispatch helpers ------------------------------------------------------------
+template <typename R, int FLUX, int MODE>
+static void launch_stage_bs(const StageParams& p, int bs, cudaStream_t st) {
+  const unsigned g = blocks_for(p.m.num_elements, bs);
+  if (bs == 64) stage_kernel<R, FLUX, MODE, 64><<<g, 64, 0, st>>>(p);
+  else if (bs == 256) stage_kernel<R, FLUX, MODE, 256><<<g, 256, 0, st>>>(p);
+  else stage_kernel<R, FLUX, MODE, 128><<<g, 128, 0, st>>>(p);
+}
+template <typename R, int MODE>
+static void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream_t st) {
+  if (flux == 0) launch_stage_bs<R, 0, MODE>(p, bs, st);
+  else if (flux == 1) launch_stage_bs<R, 1, MODE>(p, bs, st);
+  else launch_stage_bs<R, 2, MODE>(p, bs, st);
+}
+static void launch_stage(const CfdSolver* s, const StageParams& p, int mode, cudaStream_t st) {
+  const int bs = bs_of(s);
+  if (s->precision == CFD_FP64) {
+    if (mode == MODE_RHS) launch_stage_flux<double, MODE_RHS>(p, s->flux, bs, st);
+    else if (mode == MODE_LIMITED) launch_stage_flux<double, MODE_LIMITED>(p, s->flux, bs, st);
+    else launch_stage_flux<double, MODE_UNLIMITED>(p, s->flux, bs, st);
+  } else {
+    if (mode == MODE_RHS) launch_stage_flux<float, MODE_RHS>(p, s->flux, bs, st);
+    else if (mode == MODE_LIMITED) launch_stage_flux<float, MODE_LIMITED>(p, s->flux, bs, st);
+    else launch_stage_flux<float, MODE_UNLIMITED>(p, s->flux, bs, st);
+  }
+}
+template <typename R, int PHI>
+static void launch_limit_bs(const LimitParams& p, int bs, cudaStream_t st) {
+  const unsigned g = blocks_for(p.m.num_elements, bs);
+  if (bs == 64) limit_kernel<R, PHI, 64><<<g, 64, 0, st>>>(p);
+  else if (bs == 256) limit_kernel<R, PHI, 256><<<g, 256, 0, st>>>(p);
+  else limit_kernel<R, PHI, 128><<<g, 128, 0, st>>>(p);
+}
+template <typename R>
+static void launch_limit_phi(const LimitParams& p, int lim, int bs, cudaStream_t st) {
+  switch (lim) {
+    case 0: launch_limit_bs<R, 0>(p, bs, st); break;
+    case 1: launch_limit_bs<R, 1>(p, bs, st); break;
+    case 2: launch_limit_bs<R, 2>(p, bs, st); break;
+    case 3: launch_limit_bs<R, 3>(p, bs, st); break;
+    default: launch_limit_bs<R, 4>(p, bs, st); break;
+  }
+}
+static void launch_limit(const CfdSolver* s, const LimitParams& p, cudaStream_t st) {
+  if (s->precision == CFD_FP64) launch_limit_phi<double>(p, s->limiter, bs_of(s), st);
+  else launch_limit_phi<float>(p, s->limiter, bs_of(s), st);
+}
+template <typename R>
+static void launch_dt(const CfdSolver* s, const void* q, cudaStream_t st) {
+  const int bs = 128;
+  dt_kernel<R, 128><<<blocks_for(s->mesh.num_elements, bs), bs, 0, st>>>(s->mesh, (const R*)q, s->acc, s->gamma, nullptr);
+}
+static void reset_acc(const CfdSolver* s, cudaStream_t st) {
+  const int n = 3 * s->mesh.num_instances;
+  reset_acc_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, n);
+}
+
+extern "C" {
+
+int cfd_abi_version(void) { return CFD_ABI_VERSION; }
+
+int cfd_struct_sizes(int32_t* out, int32_t n) {
+  if (!out || n < 5) return fail(CFD_E_ARG, "cfd_struct_sizes: need room for 5 sizes");
+  out[0] = (int32_t)sizeof(CfdMesh);
+  out[1] = (int32_t)sizeof(CfdStageAcc);
+  out[2] = (int32_t)sizeof(CfdStepReport);
+  out[3] = (int32_t)sizeof(CfdControl);
+  out[4] = (int32_t)sizeof(CfdSolver);
+  return CFD_OK;
+}
+const char* cfd_last_error(void) { return g_err; }
+
+int cfd_pack_state(const double* q_nk4, void* q_dev, int32_t K, int32_t ld, int32_t precision, void* stream) {
+  if (!q_nk4 || !q_dev || K <= 0 || ld < K) return fail(CFD_E_ARG, "cfd_pack_state: bad arguments");
+  if (((uintptr_t)q_nk4) % 32) return fail(CFD_E_ARG, "cfd_pack_state: input must be 32-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)NP * K;
+  if (precision == CFD_FP64) pack_kernel<double><<<blocks_for(n, 256), 256, 0, st>>>(q_nk4, (double*)q_dev, K, ld);
+  else if (precision == CFD_FP32_MIXED) pack_kernel<float><<<blocks_for(n, 256), 256, 0, st>>>(q_nk4, (float*)q_dev, K, ld);
+  else return fail(CFD_E_ARG, "cfd_pack_state: unknown precision");
+  return check_launch("cfd_pack_state");
+}
+
+int cfd_unpack_state(const void* q_dev, double* q_nk4, int32_t K, int32_t ld, int32_t precision, void* stream) {
+  if (!q_nk4 || !q_dev || K <= 0 || ld < K) return fail(CFD_E_ARG, "cfd_unpack_state: bad arguments");
+  if (((uintptr_t)q_nk4) % 32) return fail(CFD_E_ARG, "cfd_unpack_state: output must be 32-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)NP * K;
+  if (precision == CFD_FP64) unpack_kernel<double><<<blocks_for(n, 256), 256, 0, st>>>((const double*)q_dev, q_nk4, K, ld);
+  else if (precision == CFD_FP32_MIXED) unpack_kernel<float><<<blocks_for(n, 256), 256, 0, st>>>((const float*)q_dev, q_nk4, K, ld);
+  else return fail(CFD_E_ARG, "cfd_unpack_state: unknown precision");
+  return check_launch("cfd_unpack_state");
+}
+
+int cfd_rhs(const CfdSolver* s, const void* q, void* rhs, double* bflux, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q || !rhs || !bflux) return fail(CFD_E_ARG, "cfd_rhs: null pointer");
+  if (q == rhs) return fail(CFD_E_ARG, "cfd_rhs: rhs must not alias q");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(bflux, 0, sizeof(double) * 4 * s->mesh.num_instances, st) != cudaSuccess)
+    return check_launch("cfd_rhs: memset");
+  StageParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = s->mesh;
+  p.gamma = s->gamma;
+  p.q_in = q;
+  p.q_out = rhs;
+  p.bflux_out = bflux;
+  launch_stage(s, p, MODE_RHS, st);
+  return check_launch("cfd_rhs");
+}
+
+int cfd_limit(const CfdSolver* s, const void* q_in, void* q_out, int32_t* troubled, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q_in || !q_out || !troubled || !s->averages || !s->element_aux) return fail(CFD_E_ARG, "cfd_limit: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(troubled, 0, sizeof(int32_t) * s->mesh.num_instances, st) != cudaSuccess)
+    return check_launch("cfd_limit: memset");
+  const int bs = 128;
+  const unsigned g = blocks_for(s->mesh.num_elements, bs);
+  if (s->precision == CFD_FP64)
+    prep_kernel<double, 128><<<g, bs, 0, st>>>(s->mesh, (const double*)q_in, (double*)q_out, s->averages, s->element_aux, s->gamma);
+  else
+    prep_kernel<float, 128><<<g, bs, 0, st>>>(s->mesh, (const float*)q_in, (float*)q_out, s->averages, s->element_aux, s->gamma);
+  LimitParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = s->mesh;
+  p.stage_idx = 0;
+  p.q_io = q_out;
+  p.gamma = s->gamma;
+  p.avg = s->averages;
+  p.aux = s->element_aux;
+  p.troubled_out = troubled;
+  launch_limit(s, p, st);
+  return check_launch("cfd_limit");
+}
+
+int cfd_time_step(const CfdSolver* s, const void* q, double* dt, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q || !dt || !s->acc) return fail(CFD_E_ARG, "cfd_time_step: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  reset_acc(s, st);
+  if (s->precision == CFD_FP64) launch_dt<double>(s, q, st);
+  else launch_dt<float>(s, q, st);
+  const int n = s->mesh.num_instances;
+  dt_out_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, dt, n, s->cfl);
+  return check_launch("cfd_time_step");
+}
+
+int cfd_check_state(const CfdSolver* s, const void* q, double* out, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q || !out || !s->acc) return fail(CFD_E_ARG, "cfd_check_state: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  reset_acc(s, st);
+  if (s->precision == CFD_FP64) launch_dt<double>(s, q, st);
+  else launch_dt<float>(s, q, st);
+  const int n = s->mesh.num_instances;
+  check_out_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, out, n);
+  return check_launch("cfd_check_state");
+}
+
+int cfd_cell_averages(const CfdSolver* s, const void* q, double* avg, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q || !avg) return fail(CFD_E_ARG, "cfd_cell_averages: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned g = blocks_for(s->mesh.num_elements, 128);
+  if (s->precision == CFD_FP64) averages_kernel<double><<<g, 128, 0, st>>>(s->mesh, (const double*)q, avg, nullptr);
+  else averages_kernel<float><<<g, 128, 0, st>>>(s->mesh, (const float*)q, avg, nullptr);
+  return check_launch("cfd_cell_averages");
+}
+
+int cfd_integrate(const CfdSolver* s, const void* q, double* integral, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q || !integral) return fail(CFD_E_ARG, "cfd_integrate: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(integral, 0, sizeof(double) * 4 * s->mesh.num_instances, st) != cudaSuccess)
+    return check_launch("cfd_integrate: memset");
+  const unsigned g = blocks_for(s->mesh.num_elements, 128);
+  if (s->precision == CFD_FP64) averages_kernel<double><<<g, 128, 0, st>>>(s->mesh, (const double*)q, nullptr, integral);
+  else averages_kernel<float><<<g, 128, 0, st>>>(s->mesh, (const float*)q, nullptr, integral);
+  return check_launch("cfd_integrate");
+}
+
+int cfd_rk3_attempt(const CfdSolver* s, void* x0, void* x1, void* stage, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!x0 || !x1 || !stage || !s->acc || !s->control || !s->report) return fail(CFD_E_ARG, "cfd_rk3_attempt: null pointer");
+  const bool limited = s->limiter != CFD_LIMITER_UNLIMITED;
+  if (limited && (!s->averages || !s->element_aux)) return fail(CFD_E_ARG, "cfd_rk3_attempt: scratch missing");
+  if (x0 == x1 || x0 == stage || x1 == stage) return fail(CFD_E_ARG, "cfd_rk3_attempt: state buffers must be distinct");
+  cudaStream_t st = (cudaStream_t)stream;
+  reset_acc(s, st);
+  StageParams p;
+  memset(&p, 0, sizeof(p));
+  p.m = s->mesh;
+  p.ctl = s->control;
+  p.x0 = x0;
+  p.x1 = x1;
+  p.stage = stage;
+  p.gamma = s->gamma;
+  p.avg = s->averages;
+  p.aux = s->element_aux;
+  p.acc = s->acc;
+  LimitParams lp;
+  memset(&lp, 0, sizeof(lp));
+  lp.m = s->mesh;
+  lp.ctl = s->control;
+  lp.x0 = x0;
+  lp.x1 = x1;
+  lp.stage = stage;
+  lp.gamma = s->gamma;
+  lp.avg = s->averages;
+  lp.aux = s->element_aux;
+  lp.acc = s->acc;
+  for (int k = 1; k <= 3; ++k) {
+    p.stage_idx = k;
+    launch_stage(s, p, limited ? MODE_LIMITED : MODE_UNLIMITED, st);
+    if (limited) {
+      lp.stage_idx = k;
+      launch_limit(s, lp, st);
+    }
+  }
+  const int n = s->mesh.num_instances;
+  report_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, s->control, s->report, n, s->cfl);
+  return check_launch("cfd_rk3_attempt");
+}
+
+int cfd_run_control(const CfdSolver* s, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!s->control || !s->report) return fail(CFD_E_ARG, "cfd_run_control: null pointer");
+  const int n = s->mesh.num_instances;
+  run_control_kernel<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(s->control, s->report, n, s->max_rejections);
+  return check_launch("cfd_run_control");
+}
+
+int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!x0 || !final_time || !s->control || !s->acc) return fail(CFD_E_ARG, "cfd_run_init: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  reset_acc(s, st);
+  if (s->precision == CFD_FP64) launch_dt<double>(s, x0, st);
+  else launch_dt<float>(s, x0, st);
+  const int n = s->mesh.num_instances;
+  run_init_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->control, s->acc, final_time, n, s->cfl);
+  return check_launch("cfd_run_init");
+}
+
+int cfd_interface_flux(int32_t flux, int32_t n, const double* q_minus, const double* q_plus, const double* nx,
+                       const double* ny, double gamma, double* out, void* stream) {
+  if (n < 0 || (n > 0 && (!q_minus || !q_plus || !nx || !ny || !out))) return fail(CFD_E_ARG, "cfd_interface_flux: bad arguments");
+  if (n == 0) return CFD_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned g = blocks_for(n, 128);
+  if (flux == 0) flux_pointwise_kernel<0><<<g, 128, 0, st>>>(n, q_minus, q_plus, nx, ny, gamma, out);
+  else if (flux == 1) flux_pointwise_kernel<1><<<g, 128, 0, st>>>(n, q_minus, q_plus, nx, ny, gamma, out);
+  else if (flux == 2) flux_pointwise_kernel<2><<<g, 128, 0, st>>>(n, q_minus, q_plus, nx, ny, gamma, out);
+  else return fail(CFD_E_ARG, "cfd_interface_flux: unknown flux id");
+  return check_launch("cfd_interface_flux");
+}
+
+int cfd_limiter_phi(int32_t limiter, int32_t n, const double* r, double* out, void* stream) {
+  if (n < 0 || (n > 0 && (!r || !out))) return fail(CFD_E_ARG, "cfd_limiter_phi: bad arguments");
+  if (n == 0) return CFD_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned g = blocks_for(n, 128);
+  switch (limiter) {
+    case 0: phi_pointwise_kernel<0><<<g, 128, 0, st>>>(n, r, out); break;
+    case 1: phi_pointwise_kernel<1><<<g, 128, 0, st>>>(n, r, out); break;
+    case 2: phi_pointwise_kernel<2><<<g, 128, 0, st>>>(n, r, out); break;
+    case 3: phi_pointwise_kernel<3><<<g, 128, 0, st>>>(n, r, out); break;
+    case 4: phi_pointwise_kernel<4><<<g, 128, 0, st>>>(n, r, out); break;
+    default: return fail(CFD_E_ARG, "cfd_limiter_phi: unknown limiter id");
+  }
+  return check_launch("cfd_limiter_phi");
+}
+
+}  // extern "C"

@@ -1,0 +1,227 @@
+"""Device tables of the DG operator and limiter, in the kernels' layout.
+
+Host-side, built once per solver (CFD-demo builds the equivalent arrays in
+src/cfd_demo/dg.py:76-116 and src/cfd_demo/limiting.py:51-121, in its own
+(3 Nfp, K) face-node layout). Here every table is element-major with a padded
+leading dimension ``ld`` so that a warp's loads of one field are contiguous:
+
+    metric     [4][ld]  rx, ry, sx, sy                         float64 (+ float32 copy)
+    face_geo   [9][ld]  nx_f, ny_f, sJ_f / J for faces f=0,1,2 float64 (+ float32 copy)
+    face_hlen  [3][ld]  half edge lengths (boundary-flux weights)
+    dt_geo     [ld]     min_e 2|K| / ((N+1)^2 |e|)             (time_integration.py:32-34)
+    jacobian   [ld]     J = |K| / 2
+    cs_coef    [6][ld]  Cockburn-Shu alpha_f, beta_f           float64 (+ float32 copy)
+    neighbor   [3][ld]  neighbour element, or fixed-state row   int32
+    face_info  [ld]     per face 8 bits: kind | nbr face << 2 | partner face << 4
+    instance   [ld]     instance id (batched meshes only)       int32
+    bc_states  [rows][4] fixed exterior states                 float64
+
+Several meshes ("instances") can be concatenated into one table set; element
+and neighbour indices are then global.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+from .boundary import FIXED_STATE, SLIP_WALL
+from .mesh import MeshConnectivity, TriangleMesh, element_geometry, node_coordinates
+
+COEFFICIENT_TOLERANCE = 1e-12  # limiting.py:31
+LD_ALIGN = 64
+
+
+def padded_ld(k: int) -> int:
+    return ((k + LD_ALIGN - 1) // LD_ALIGN) * LD_ALIGN
+
+
+def resolve_boundary_conditions(connectivity: MeshConnectivity, boundary_conditions) -> tuple[np.ndarray, np.ndarray]:
+    """Per-face kinds (K, 3) and fixed states (K, 3, 4) (dg.py:52-73)."""
+    tags = set(connectivity.boundary_tags)
+    missing = sorted(tags - set(boundary_conditions))
+    if missing:
+        raise ValueError(f"Boundary tags without a boundary condition: {missing}.")
+    unknown = sorted(set(boundary_conditions) - tags)
+    if unknown:
+        raise ValueError(f"Boundary conditions for tags that are not in the mesh: {unknown}.")
+    kind = np.zeros(connectivity.face_tag.shape, dtype=np.int32)
+    state = np.zeros(connectivity.face_tag.shape + (4,))
+    for ti, tag in enumerate(connectivity.boundary_tags):
+        bc = boundary_conditions[tag]
+        mask = connectivity.face_tag == ti
+        kind[mask] = bc.kind
+        if bc.kind == FIXED_STATE:
+            state[mask] = bc.state
+        elif bc.kind != SLIP_WALL:
+            raise ValueError(f"Unsupported boundary condition for tag {tag!r}: {bc!r}.")
+    return kind, state
+
+
+def neighbor_coefficients(connectivity: MeshConnectivity, geometry) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Nonnegative Cockburn-Shu coefficients per face, (K, 3) each
+    (limiting.py:51-94): m_i - b0 = alpha (b_i - b0) + beta (b_j - b0) with
+    the first partner face j in (i+1, i+2) that gives alpha, beta >= -tol;
+    boundary neighbours use the centroid reflected across the face."""
+    cen, mid, nrm = geometry.centroid, geometry.face_midpoint, geometry.normal
+    nb = connectivity.neighbor_element
+    off = np.sum((mid - cen[:, None, :]) * nrm, axis=-1, keepdims=True)
+    ncen = np.where((nb >= 0)[..., None], cen[np.maximum(nb, 0)], cen[:, None, :] + 2.0 * off * nrm)
+    d = ncen - cen[:, None, :]
+    t = mid - cen[:, None, :]
+    k = cen.shape[0]
+    alpha = np.zeros((k, 3))
+    beta = np.zeros((k, 3))
+    partner = np.full((k, 3), -1, dtype=np.int64)
+    for f in range(3):
+        for shift in (1, 2):
+            o = (f + shift) % 3
+            di, dj, tt = d[:, f], d[:, o], t[:, f]
+            det = di[:, 0] * dj[:, 1] - di[:, 1] * dj[:, 0]
+            safe = np.where(det == 0.0, 1.0, det)
+            a = (tt[:, 0] * dj[:, 1] - tt[:, 1] * dj[:, 0]) / safe
+            b = (di[:, 0] * tt[:, 1] - di[:, 1] * tt[:, 0]) / safe
+            pick = (det != 0.0) & (a >= -COEFFICIENT_TOLERANCE) & (b >= -COEFFICIENT_TOLERANCE) & (partner[:, f] < 0)
+            alpha[pick, f] = np.maximum(a[pick], 0.0)
+            beta[pick, f] = np.maximum(b[pick], 0.0)
+            partner[pick, f] = o
+    if np.any(partner < 0):
+        e, f = np.argwhere(partner < 0)[0]
+        raise ValueError(f"No nonnegative Cockburn-Shu neighbor coefficients for face {f} of element {e}.")
+    return alpha, beta, partner
+
+
+def check_face_pairing(mesh: TriangleMesh, connectivity: MeshConnectivity, reference, relative_tolerance=1e-9) -> None:
+    """Check by coordinates that face node k of face f meets node 4-k (or k)
+    of the neighbour's face, the rule the kernels use (mesh.py:254-291 pairs
+    the nodes by coordinates)."""
+    x, y = node_coordinates(mesh, reference.r, reference.s)
+    fn = reference.face_nodes
+    nfp = fn.shape[1]
+    lengths = element_geometry(mesh).edge_length
+    for f in range(3):
+        el = np.flatnonzero(connectivity.neighbor_element[:, f] >= 0)
+        if el.size == 0:
+            continue
+        nb = connectivity.neighbor_element[el, f]
+        nf = connectivity.neighbor_face[el, f]
+        same = (f == 2) != (nf == 2)
+        for k in range(nfp):
+            kk = np.where(same, k, nfp - 1 - k)
+            pn = fn[nf, kk]
+            dist = np.hypot(x[fn[f, k], el] - x[pn, nb], y[fn[f, k], el] - y[pn, nb])
+            if np.any(dist > relative_tolerance * lengths[el, f]):
+                raise ValueError("Neighboring face nodes do not coincide; the mesh is not conforming.")
+
+
+@dataclass
+class HostTables:
+    """One instance's tables on the host (float64 / int32), before upload."""
+
+    num_elements: int
+    metric: np.ndarray  # (4, K)
+    face_geo: np.ndarray  # (9, K)
+    face_hlen: np.ndarray  # (3, K)
+    dt_geo: np.ndarray  # (K,)
+    jacobian: np.ndarray  # (K,)
+    cs_coef: np.ndarray  # (6, K)
+    neighbor: np.ndarray  # (3, K) int32 (local element ids, or local bc rows)
+    face_info: np.ndarray  # (K,) int32
+    bc_states: np.ndarray  # (rows, 4)
+    interior: np.ndarray = field(default=None)  # (3, K) bool
+
+
+def host_tables(mesh: TriangleMesh, connectivity: MeshConnectivity, geometry, reference, kind: np.ndarray,
+                state: np.ndarray, degree: int = 4) -> HostTables:
+    k = mesh.num_elements
+    check_face_pairing(mesh, connectivity, reference)
+    alpha, beta, partner = neighbor_coefficients(connectivity, geometry)
+    # fixed-state rows: one per distinct exterior state
+    fixed = kind == FIXED_STATE
+    rows, inverse = (np.unique(state[fixed], axis=0, return_inverse=True) if fixed.any()
+                     else (np.zeros((0, 4)), np.zeros(0, dtype=np.int64)))
+    nbr = np.where(connectivity.neighbor_element >= 0, connectivity.neighbor_element, 0).astype(np.int64)
+    nbr[fixed] = inverse.reshape(-1)
+    nface = np.where(connectivity.neighbor_face >= 0, connectivity.neighbor_face, 0)
+    info = np.zeros(k, dtype=np.int64)
+    for f in range(3):
+        field8 = kind[:, f].astype(np.int64) | (nface[:, f] << 2) | (partner[:, f] << 4)
+        info |= field8 << (8 * f)
+    fscale = 0.5 * geometry.edge_length / geometry.jacobian[:, None]  # dg.py:99
+    face_geo = np.empty((9, k))
+    for f in range(3):
+        face_geo[3 * f] = geometry.normal[:, f, 0]
+        face_geo[3 * f + 1] = geometry.normal[:, f, 1]
+        face_geo[3 * f + 2] = fscale[:, f]
+    dt_geo = np.min(2.0 * geometry.area[:, None] / ((degree + 1) ** 2 * geometry.edge_length), axis=1)
+    return HostTables(
+        num_elements=k,
+        metric=np.stack([geometry.rx, geometry.ry, geometry.sx, geometry.sy]),
+        face_geo=face_geo,
+        face_hlen=(0.5 * geometry.edge_length).T.copy(),
+        dt_geo=dt_geo,
+        jacobian=np.asarray(geometry.jacobian, dtype=np.float64),
+        cs_coef=np.concatenate([alpha.T, beta.T]),
+        neighbor=nbr.T.astype(np.int32),
+        face_info=info.astype(np.int32),
+        bc_states=np.asarray(rows, dtype=np.float64).reshape(-1, 4),
+        interior=(connectivity.neighbor_element >= 0).T,
+    )
+
+
+class DeviceTables:
+    """Mesh tables of one or more instances uploaded as torch tensors, plus the
+    ``CfdMesh`` struct pointing at them. Keeps the tensors alive."""
+
+    def __init__(self, parts: list[HostTables], device, precision: int):
+        import torch
+
+        self.device = torch.device(device)
+        sizes = [p.num_elements for p in parts]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        k = int(self.offsets[-1])
+        ld = padded_ld(k)
+        self.num_elements, self.ld, self.num_instances = k, ld, len(parts)
+        bc_off = np.concatenate([[0], np.cumsum([len(p.bc_states) for p in parts])]).astype(np.int64)
+
+        def cat(name, rows):
+            out = np.zeros((rows, ld), dtype=getattr(parts[0], name).dtype)
+            for p, o in zip(parts, self.offsets[:-1]):
+                out[:, o:o + p.num_elements] = getattr(p, name).reshape(rows, -1)
+            return out
+
+        metric, face_geo, face_hlen = cat("metric", 4), cat("face_geo", 9), cat("face_hlen", 3)
+        cs = cat("cs_coef", 6)
+        dt_geo, jac = cat("dt_geo", 1)[0], cat("jacobian", 1)[0]
+        nbr = np.zeros((3, ld), dtype=np.int32)
+        info = np.zeros(ld, dtype=np.int32)
+        inst = np.zeros(ld, dtype=np.int32)
+        for i, (p, o) in enumerate(zip(parts, self.offsets[:-1])):
+            kinds = np.stack([(p.face_info >> (8 * f)) & 3 for f in range(3)])
+            local = p.neighbor.astype(np.int64)
+            glob = np.where(kinds == FIXED_STATE, local + bc_off[i], np.where(kinds == 0, local + o, 0))
+            nbr[:, o:o + p.num_elements] = glob
+            info[o:o + p.num_elements] = p.face_info
+            inst[o:o + p.num_elements] = i
+        bcs = np.concatenate([p.bc_states for p in parts]) if bc_off[-1] else np.zeros((1, 4))
+
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(self.device)  # noqa: E731
+        self.metric, self.face_geo, self.face_hlen = t(metric), t(face_geo), t(face_hlen)
+        self.dt_geo, self.jacobian, self.cs_coef = t(dt_geo), t(jac), t(cs)
+        self.neighbor, self.face_info = t(nbr), t(info)
+        self.instance = t(inst) if len(parts) > 1 else None
+        self.bc_states = t(bcs)
+        self.precision = precision
+        if precision == _native.CFD_FP32_MIXED:
+            self.metric32 = self.metric.float().contiguous()
+            self.face_geo32 = self.face_geo.float().contiguous()
+            self.cs_coef32 = self.cs_coef.float().contiguous()
+        else:
+            self.metric32 = self.face_geo32 = self.cs_coef32 = None
+        ptr = lambda x: None if x is None else x.data_ptr()  # noqa: E731
+        self.struct = _native.CfdMesh(
+            k, ld, len(parts), 0, ptr(self.metric), ptr(self.face_geo), ptr(self.face_hlen), ptr(self.dt_geo),
+            ptr(self.jacobian), ptr(self.cs_coef), ptr(self.neighbor), ptr(self.face_info), ptr(self.instance),
+            ptr(self.bc_states), ptr(self.metric32), ptr(self.face_geo32), ptr(self.cs_coef32))

@@ -1,0 +1,233 @@
+/*
+ * cfd_b200.h — C ABI of the B200 (sm_100a) kernels for the degree-4 nodal DG
+ * Euler hot path of CFD-demo.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), returns 0 on success or a negative CFD_E* code, never
+ * allocates device memory, and never synchronises the stream. The message of
+ * the last failure on the calling thread is in cfd_last_error().
+ *
+ * Device state layout ("element-major SoA"): a state with K elements is an
+ * array q[(c * 15 + j) * ld + e] for conserved variable c in (rho, rho u,
+ * rho v, E), node j in 0..14 (the reference triangle's node order) and element
+ * e in 0..K-1, with ld >= K. The reference's host layout (Np, K, 4) is
+ * converted by cfd_pack_state / cfd_unpack_state. Precision CFD_FP64 stores
+ * doubles; CFD_FP32_MIXED stores floats (averages, positivity pressure
+ * recovery and all global reductions stay in double).
+ *
+ * Reference interfaces replaced (paths relative to the CFD-demo project):
+ *   cfd_rhs            src/cfd_demo/dg.py:140-165          dg_rhs
+ *   cfd_limit          src/cfd_demo/limiting.py:203-216    apply_limiters
+ *   cfd_time_step      src/cfd_demo/time_integration.py:37-41  stable_time_step
+ *   cfd_rk3_attempt    src/cfd_demo/time_integration.py:44-84  ssp_rk3_step
+ *   cfd_run_control    src/cfd_demo/solver.py:167-216       EulerSolver.run loop body
+ *   cfd_cell_averages  src/cfd_demo/dg.py:168-171          cell_averages
+ *   cfd_integrate      src/cfd_demo/dg.py:174-176          domain_integral
+ *   cfd_check_state    src/cfd_demo/solver.py:170-176      initial admissibility
+ *   cfd_interface_flux src/cfd_demo/fluxes.py:28-159       rusanov / roe / hllc
+ *   cfd_limiter_phi    src/cfd_demo/limiters.py:16-57      phi(r)
+ */
+#ifndef CFD_B200_H
+#define CFD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFD_ABI_VERSION 1
+
+/* error codes */
+#define CFD_OK 0
+#define CFD_E_ARG (-1)     /* invalid argument (null pointer, bad id, bad size) */
+#define CFD_E_CUDA (-2)    /* a CUDA launch or API call failed */
+
+/* interface flux ids (fluxes.py:146-150) */
+#define CFD_FLUX_RUSANOV 0
+#define CFD_FLUX_ROE 1
+#define CFD_FLUX_HLLC 2
+
+/* limiter ids (limiters.py:42-48) */
+#define CFD_LIMITER_MINMOD 0
+#define CFD_LIMITER_MC 1
+#define CFD_LIMITER_VAN_LEER 2
+#define CFD_LIMITER_SUPERBEE 3
+#define CFD_LIMITER_UNLIMITED 4
+
+/* precision ids */
+#define CFD_FP64 0
+#define CFD_FP32_MIXED 1
+
+/* boundary kinds (boundary.py:13-14); 0 = interior face */
+#define CFD_FACE_INTERIOR 0
+#define CFD_FACE_SLIP_WALL 1
+#define CFD_FACE_FIXED_STATE 2
+
+/* run status (CfdControl.status) */
+#define CFD_RUN_ACTIVE 0
+#define CFD_RUN_DONE 1
+#define CFD_RUN_BAD_DT (-1)
+#define CFD_RUN_REJECTED (-2)
+
+/*
+ * Mesh tables in device memory, one entry per element unless stated; every
+ * per-element array has leading dimension ld. Several instances (meshes) may
+ * be concatenated: element e belongs to instance instance[e] (NULL: one
+ * instance), and neighbour indices are global element indices.
+ *
+ * face_info[e] packs, for face f = 0, 1, 2, the 8-bit field
+ * (face_info >> 8 f) & 0xff =
+ *     kind (bits 0-1, CFD_FACE_*) | neighbour's local face (bits 2-3)
+ *   | Cockburn-Shu partner face (bits 4-5) | reserved (bits 6-7).
+ * Face node k of face f meets node 4-k of the neighbour's face g when f and g
+ * are both 2 or both not 2, and node k otherwise (the face-2 nodes run against
+ * the counterclockwise direction); the host checks this rule by coordinates.
+ * neighbor[f * ld + e] is the neighbour element across face f for interior
+ * faces and, for fixed-state faces, the row of bc_states (4 doubles) holding
+ * the exterior state.
+ */
+typedef struct CfdMesh {
+    int32_t num_elements;  /* K: elements of all instances */
+    int32_t ld;            /* leading dimension, >= num_elements */
+    int32_t num_instances; /* >= 1 */
+    int32_t reserved0;
+    const double* metric;    /* [4][ld]  rx, ry, sx, sy */
+    const double* face_geo;  /* [9][ld]  nx_f, ny_f, Fscale_f (= sJ/J) for f = 0,1,2 */
+    const double* face_hlen; /* [3][ld]  half edge length (boundary-flux weights) */
+    const double* dt_geo;    /* [ld]     min_e 2|K| / ((N+1)^2 |e|) */
+    const double* jacobian;  /* [ld]     J = |K| / 2 */
+    const double* cs_coef;   /* [6][ld]  alpha_f, beta_f (limiting.py:51-94) */
+    const int32_t* neighbor; /* [3][ld] */
+    const int32_t* face_info;/* [ld] */
+    const int32_t* instance; /* [ld] instance of each element, or NULL */
+    const double* bc_states; /* [rows][4] fixed exterior states */
+    const float* metric32;   /* FP32 copies for CFD_FP32_MIXED, else NULL */
+    const float* face_geo32;
+    const float* cs_coef32;
+} CfdMesh;
+
+/* Per instance and per RK stage reduction slots (zeroed by cfd_rk3_attempt). */
+typedef struct CfdStageAcc {
+    double boundary_flux[4];        /* sum of w * sJ * Fhat over boundary face nodes */
+    unsigned long long min_rho_key; /* ordered key of the minimum nodal density */
+    unsigned long long min_p_key;   /* ordered key of the minimum nodal pressure */
+    unsigned long long dt_key;      /* ordered key of min_K dt_geo / lambda_K (stage 3) */
+    int32_t troubled;               /* troubled-cell count */
+    int32_t flags;                  /* bit 0: non-finite value; bit 1: average rho or p <= 0 */
+} CfdStageAcc;
+
+/* StepReport of time_integration.py:22-29 (written by cfd_rk3_attempt). */
+typedef struct CfdStepReport {
+    double boundary_flux[4]; /* dt (B0/6 + B1/6 + 2 B2/3) */
+    double min_density;
+    double min_pressure;
+    double dt;               /* the step size used */
+    double dt_next;          /* CFL step of the new state (time_step(q_new)) */
+    int32_t admissible;
+    int32_t troubled_cells;
+    int32_t reserved[2];
+} CfdStepReport;
+
+/* Host run-loop state of solver.py:177-204, kept on the device per instance. */
+typedef struct CfdControl {
+    double time;
+    double final_time;
+    double dt;            /* step size of the current attempt */
+    double flux_integral[4];
+    double min_density;
+    double min_pressure;
+    int32_t steps;
+    int32_t rejected;
+    int32_t attempts;     /* failed attempts of the current step */
+    int32_t max_troubled;
+    int32_t parity;       /* which of (x0, x1) holds the current state */
+    int32_t status;       /* CFD_RUN_* */
+    int32_t reaches_end;
+    int32_t reserved;
+} CfdControl;
+
+/* Solver description: mesh + configuration + caller-owned scratch. */
+typedef struct CfdSolver {
+    CfdMesh mesh;
+    int32_t flux;          /* CFD_FLUX_* */
+    int32_t limiter;       /* CFD_LIMITER_* */
+    int32_t precision;     /* CFD_FP64 | CFD_FP32_MIXED */
+    int32_t max_rejections;
+    double gamma;
+    double cfl;
+    /* scratch, caller-allocated device memory */
+    double* averages;      /* [4][ld] stage cell averages (double in both precisions) */
+    double* element_aux;   /* [3][ld] per-element min rho, min p, lambda (limited runs) */
+    CfdStageAcc* acc;      /* [num_instances][3] */
+    CfdStepReport* report; /* [num_instances] */
+    CfdControl* control;   /* [num_instances] */
+    int32_t block_size;    /* threads per block of the element kernels (64, 128, 256); 0 = default */
+    int32_t reserved1;
+} CfdSolver;
+
+/* ---- library ------------------------------------------------------------- */
+int cfd_abi_version(void);
+/* sizeof CfdMesh, CfdStageAcc, CfdStepReport, CfdControl, CfdSolver (host only;
+ * lets a binding check its struct layouts). */
+int cfd_struct_sizes(int32_t* out, int32_t n);
+const char* cfd_last_error(void);
+
+/* Layout conversion: host layout (Np, K, 4) double <-> device layout of
+ * `precision`. Both pointers are device memory. */
+int cfd_pack_state(const double* q_nk4, void* q_dev, int32_t K, int32_t ld, int32_t precision, void* stream);
+int cfd_unpack_state(const void* q_dev, double* q_nk4, int32_t K, int32_t ld, int32_t precision, void* stream);
+
+/* ---- operators (one instance or all instances at once) --------------------
+ * cfd_rhs: rhs = L(q) (dg.py:140-165) and, per instance, the boundary flux
+ * integral bflux[inst*4 + c] (zeroed by the call). */
+int cfd_rhs(const CfdSolver* s, const void* q, void* rhs, double* bflux, void* stream);
+
+/* cfd_limit: apply_limiters (limiting.py:203-216) from q_in to q_out (may
+ * alias); troubled[inst] receives the troubled-cell count. */
+int cfd_limit(const CfdSolver* s, const void* q_in, void* q_out, int32_t* troubled, void* stream);
+
+/* cfd_time_step: dt[inst] = cfl * min_K dt_geo / max_nodes(|u| + c). */
+int cfd_time_step(const CfdSolver* s, const void* q, double* dt, void* stream);
+
+/* cfd_cell_averages: avg[c * ld + e] (double); cfd_integrate: integral[inst*4 + c]. */
+int cfd_cell_averages(const CfdSolver* s, const void* q, double* avg, void* stream);
+int cfd_integrate(const CfdSolver* s, const void* q, double* integral, void* stream);
+
+/* cfd_check_state: out[inst*3 + {0,1,2}] = min nodal density, min nodal
+ * pressure, 1.0 if every value is finite else 0.0. */
+int cfd_check_state(const CfdSolver* s, const void* q, double* out, void* stream);
+
+/*
+ * cfd_rk3_attempt: one SSP-RK3 step attempt (time_integration.py:44-84) for
+ * every active instance. The current state of instance i is x0 if
+ * control[i].parity == 0 else x1; the new state goes to the other buffer;
+ * stage is a third state buffer. dt is control[i].dt. Writes report[i]
+ * (including dt_next, the CFL step of the new state). Instances whose
+ * control.status != CFD_RUN_ACTIVE are skipped. The parity is NOT flipped:
+ * cfd_run_control (or the caller) accepts the step.
+ */
+int cfd_rk3_attempt(const CfdSolver* s, void* x0, void* x1, void* stage, void* stream);
+
+/*
+ * cfd_run_control: the body of the reference's run loop (solver.py:180-204)
+ * after an attempt, per instance: accept (flip parity, advance time, count,
+ * accumulate boundary flux and minima, take dt_next clipped to the final
+ * time) or reject (halve dt, up to max_rejections), setting status to DONE or
+ * an error when the loop would end.
+ */
+int cfd_run_control(const CfdSolver* s, void* stream);
+
+/* cfd_run_init: control[i] = {time 0, final_time[i], dt = clipped CFL step of
+ * the current state, ...}; minima start from the nodal minima of the state. */
+int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, void* stream);
+
+/* ---- pointwise physics (exercise the device functions of the fused kernels) */
+int cfd_interface_flux(int32_t flux, int32_t n, const double* q_minus, const double* q_plus,
+                       const double* nx, const double* ny, double gamma, double* out, void* stream);
+int cfd_limiter_phi(int32_t limiter, int32_t n, const double* r, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFD_B200_H */

@@ -1,0 +1,160 @@
+"""GPU parity of the sm_100a kernels (through the C ABI) against golden vectors
+made by the reference's own source and against the CPU oracle.
+
+Tolerances (plain FP64 form), "relative" = |gpu - ref| / max |ref| of the same
+conserved variable over the mesh:
+  * one RHS evaluation:                 1e-12
+  * limiters, one RK3 step:             1e-12 / 1e-11
+  * the 20x2 and 100x10 Sod runs:       1e-10 (final state), identical step
+                                        counts and troubled-cell maxima
+  * troubled-cell counts and flags:     exact
+  * pointwise interface fluxes:         1e-13 relative + 1e-13 absolute
+  * phi(r):                             bit-exact
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.golden_io import FLUXES, GAMMA, LIMITERS, case_prefixes, load
+from tests.gpu_helpers import make_solver, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def test_pointwise_fluxes_match_reference():
+    from cfd_demo_b200 import get_interface_flux
+
+    g = load("pointwise")
+    for name in FLUXES:
+        out = get_interface_flux(name)(g["q_minus"], g["q_plus"], g["nx"], g["ny"], GAMMA)
+        np.testing.assert_allclose(out, g[f"flux/{name}"], rtol=1e-13, atol=1e-13, err_msg=name)
+
+
+def test_phi_bit_exact():
+    from cfd_demo_b200 import get_limiter_function
+
+    g = load("pointwise")
+    for name in LIMITERS:
+        assert np.array_equal(get_limiter_function(name)(g["phi/r"]), g[f"phi/{name}"]), name
+
+
+@pytest.mark.parametrize("prefix", case_prefixes(load("rhs")))
+@pytest.mark.parametrize("flux", FLUXES)
+def test_rhs_matches_reference(prefix, flux):
+    g = load("rhs")
+    s = make_solver(g, prefix, flux=flux)
+    rhs, bflux = s.rhs(g[f"{prefix}/q"])
+    ref = g[f"{prefix}/rhs/{flux}"]
+    if prefix == "freestream":
+        assert np.abs(rhs).max() < 1e-11
+    else:
+        assert rel_err(rhs, ref) <= 1e-12
+    rb = g[f"{prefix}/bflux/{flux}"]
+    assert np.abs(bflux - rb).max() <= 1e-12 * max(np.abs(rb).max(), 1.0)
+
+
+@pytest.mark.parametrize("prefix", case_prefixes(load("limit")))
+@pytest.mark.parametrize("limiter", LIMITERS)
+def test_limit_matches_reference(prefix, limiter):
+    g = load("limit")
+    s = make_solver(g, prefix, limiter=limiter)
+    q = g[f"{prefix}/q"]
+    limited, count = s.limit_with_count(q)
+    assert rel_err(limited, g[f"{prefix}/limited/{limiter}"]) <= 1e-12
+    assert count == int(g[f"{prefix}/count/{limiter}"])
+    if limiter != "unlimited":
+        # the elements the limiter changed are exactly the troubled ones or
+        # the ones the positivity limiter touched
+        flags = g[f"{prefix}/troubled/{limiter}"]
+        changed = np.any(np.abs(limited - q) > 0, axis=(0, 2))
+        assert np.all(changed[flags]) or prefix == "positivity"
+    assert np.abs(s.cell_averages(q) - g[f"{prefix}/averages"]).max() <= 1e-13 * np.abs(g[f"{prefix}/averages"]).max()
+    np.testing.assert_allclose(s.integrate(q), g[f"{prefix}/integral"], rtol=1e-12, atol=1e-15)
+
+
+def test_positivity_floor_is_met_exactly():
+    """The reference's own acceptance (test_limiting_and_time.py:91-109):
+    every node ends at >= 1e-13 (1 - 1e-9) in density and pressure."""
+    from cfd_demo_b200.euler import conserved_to_primitive
+
+    g = load("limit")
+    s = make_solver(g, "positivity", limiter="unlimited")
+    q = g["positivity/q"]
+    limited = s.limit(q)
+    rho, _, _, p = conserved_to_primitive(limited, GAMMA)
+    assert rho.min() >= 1e-13 * (1.0 - 1e-9)
+    assert p.min() >= 1e-13 * (1.0 - 1e-9)
+    assert np.abs(s.cell_averages(limited) - s.cell_averages(q)).max() < 1e-12
+
+
+@pytest.mark.parametrize("flux", FLUXES)
+@pytest.mark.parametrize("limiter", LIMITERS)
+def test_step_matches_reference(flux, limiter):
+    g = load("step")
+    s = make_solver(g, "mesh", flux=flux, limiter=limiter)
+    key = f"{flux}/{limiter}"
+    assert s.time_step(g["q"]) == pytest.approx(float(g[f"{key}/dt"]), rel=1e-13)
+    qn, rep = s.step(g["q"], float(g[f"{key}/dt"]))
+    assert rel_err(qn, g[f"{key}/q_new"]) <= 1e-11
+    np.testing.assert_allclose(rep.boundary_flux, g[f"{key}/boundary_flux"], rtol=1e-11, atol=1e-15)
+    assert rep.admissible == bool(g[f"{key}/admissible"])
+    assert rep.min_density == pytest.approx(float(g[f"{key}/min_density"]), rel=1e-11)
+    assert rep.min_pressure == pytest.approx(float(g[f"{key}/min_pressure"]), rel=1e-9, abs=1e-18)
+    assert rep.troubled_cells == int(g[f"{key}/troubled_cells"])
+
+
+def _sod_like(nx, ny, flux="rusanov", limiter="minmod"):
+    from cfd_demo_b200 import EulerSolver, SolverConfig, rectangle_mesh
+    from cfd_demo_b200.cases import sod_boundaries
+
+    return EulerSolver(rectangle_mesh(nx, ny), sod_boundaries(), SolverConfig(flux=flux, limiter=limiter, gamma=GAMMA))
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_short_sod_run_matches_reference(graph):
+    g = load("sod_short")
+    s = _sod_like(20, 2)
+    res = s.run(g["initial_state"], 0.01, graph=graph)
+    assert res.steps == int(g["steps"]) and res.rejected_steps == int(g["rejected_steps"])
+    assert res.time == float(g["time"])
+    assert res.max_troubled_cells == int(g["max_troubled_cells"])
+    assert rel_err(res.state, g["state"]) <= 1e-10
+    np.testing.assert_allclose(res.boundary_flux_integral, g["boundary_flux_integral"], rtol=1e-10, atol=1e-14)
+    assert res.min_density == pytest.approx(float(g["min_density"]), rel=1e-10)
+
+
+def test_short_sod_stage_troubled_counts_match_per_step():
+    """March the golden dt sequence step by step: per-step troubled maxima
+    must match exactly (the flags are decided in the reference's op order)."""
+    g = load("sod_short")
+    s = _sod_like(20, 2)
+    q = g["initial_state"]
+    for n, dt in enumerate(g["dt"]):
+        q, rep = s.step(q, float(dt))
+        assert rep.troubled_cells == int(g["stage_troubled"][n].max()), f"step {n}"
+        assert rep.admissible
+
+
+def test_config0_sod_run_matches_reference(report):
+    """Sod 100x10 (K=2000), rusanov/minmod, t=0.2, CFL 0.5: the plain FP64
+    path against the reference run (3186 steps)."""
+    from cfd_demo_b200 import sod_shock_tube
+
+    g = load("sod_config0")
+    case = sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")
+    assert np.array_equal(case.initial_state, g["initial_state"])
+    res = case.solver.run(case.initial_state, case.final_time)
+    err = rel_err(res.state, g["state"])
+    report(f"config-0 Sod run: steps {res.steps} (ref {int(g['steps'])}), max troubled {res.max_troubled_cells} "
+           f"(ref {int(g['max_troubled_cells'])}), state rel err {err:.2e}, wall {res.wall_time:.2f} s")
+    assert res.steps == int(g["steps"])
+    assert res.rejected_steps == 0
+    assert res.time == pytest.approx(0.2, abs=1e-15)
+    assert res.max_troubled_cells == int(g["max_troubled_cells"])
+    assert err <= 1e-10
+    np.testing.assert_allclose(res.boundary_flux_integral, g["boundary_flux_integral"], rtol=1e-10, atol=1e-13)
+    assert res.min_density == pytest.approx(float(g["min_density"]), rel=1e-10)
+    defect = case.solver.integrate(res.state) - case.solver.integrate(case.initial_state) + res.boundary_flux_integral
+    assert np.abs(defect).max() <= 1e-12
