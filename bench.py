@@ -1,0 +1,445 @@
+"""Benchmark of the DG Euler RK3 step on B200 (one JSON line on rank 0).
+
+Workload (the 1M-triangle microbenchmark): [0,1]^2 meshed as 724x724 quads,
+each split into 2 triangles (K = 1,048,352, P = 4, Np = 15), interior
+vertices jittered by seeded uniform +-0.2h; per-node fields are sums of 8
+seeded random Fourier modes mapped affinely to rho in [0.5,1.5], u,v in
+[-0.5,0.5], p in [0.5,1.5]; every boundary tag is a fixed state at the mean
+state; flux=roe, limiter=unlimited (positivity still runs). A step is one full
+SSP-RK3 step: 3 fused stages, positivity, device CFL dt and the device
+run-loop control. DOF = K * Np solution nodes (4 conserved scalars each).
+
+Headline `value`: DOF-steps/s of the FP32-mixed form with the state resident
+in HBM; `fp64` holds the plain FP64 form on the same workload; `l1_rho_vs_fp64`
+is the domain-averaged L1 density difference after the timed steps; `e2e`
+runs EulerSolver.run() from a pinned host state to a host result.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (torchrun, one rank per GPU) every rank advances its own
+replica of the workload (weak scaling; the path needs no data exchange
+between replicas) and the timing is the maximum over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-steps/s FP32-mixed vs FP64 plain at L1(rho)<=1e-5; adjoint/forward time"
+NX = 724
+JITTER = 0.2
+MESH_SEED = 20261203
+FIELD_SEED = 7
+NP_NODES = 15
+FALLBACK_HBM_GBS = 6650.0
+# Algorithmic bytes per element per RK3 step of the three stage launches:
+# state read + write per stage, the stage base state in stages 2-3, and the
+# per-element geometry (4 metric + 9 face values + face_info + 3 neighbour ids,
+# + dt_geo in stage 3). Neighbour-trace gathers are counted once (in the
+# neighbour's own read).
+def stage_bytes(real_bytes: int) -> list[int]:
+    state = 60 * real_bytes
+    geo = 13 * real_bytes + 4 + 12
+    return [2 * state + geo, 3 * state + geo, 3 * state + geo + 8]
+
+
+# ---------------------------------------------------------------- workload ---
+def fourier_field(x, y, rng, lo, hi, xp):
+    """Sum of 8 random Fourier modes, mapped affinely onto [lo, hi]."""
+    f = xp.zeros_like(x)
+    for _ in range(8):
+        kx, ky = rng.integers(1, 5, size=2)
+        amp = rng.uniform(0.3, 1.0)
+        ph = rng.uniform(0.0, 2 * math.pi)
+        f = f + amp * xp.cos(2 * math.pi * (float(kx) * x + float(ky) * y) + ph)
+    fmin, fmax = f.min(), f.max()
+    return lo + (hi - lo) * (f - fmin) / (fmax - fmin)
+
+
+def make_workload(nx: int = NX, precision: str = "fp32_mixed", device="cuda"):
+    """(solver, initial state as a device (Np, K, 4) float64 tensor)."""
+    import torch
+
+    from cfd_demo_b200 import EulerSolver, FixedState, SolverConfig, jittered_rectangle_mesh
+
+    mesh = jittered_rectangle_mesh(nx, nx, JITTER, MESH_SEED)
+    mean = FixedState.from_primitive(1.0, 0.0, 0.0, 1.0, 1.4)
+    bcs = {t: mean for t in ("left", "right", "bottom", "top")}
+    solver = EulerSolver(mesh, bcs, SolverConfig(flux="roe", limiter="unlimited", gamma=1.4, precision=precision),
+                         device=device)
+    return solver, initial_state(solver, device)
+
+
+def initial_state(solver, device="cuda"):
+    import torch
+
+    x, y = solver.node_coordinates()
+    xt = torch.as_tensor(x, device=device)
+    yt = torch.as_tensor(y, device=device)
+    rng = np.random.default_rng(FIELD_SEED)
+    rho = fourier_field(xt, yt, rng, 0.5, 1.5, torch)
+    u = fourier_field(xt, yt, rng, -0.5, 0.5, torch)
+    v = fourier_field(xt, yt, rng, -0.5, 0.5, torch)
+    p = fourier_field(xt, yt, rng, 0.5, 1.5, torch)
+    e = p / 0.4 + 0.5 * rho * (u * u + v * v)
+    return torch.stack([rho, rho * u, rho * v, e], dim=-1).contiguous()
+
+
+# ----------------------------------------------------------- CPU baseline ---
+def _oracle_sample_worker(args):
+    """Time `steps` oracle RK3 steps (after one warm-up) on an nx x nx sample
+    of the workload; returns (elements, steps, seconds)."""
+    nx, steps = args
+    sys.path.insert(0, ROOT)
+    import oracle
+    from oracle.physics import FixedState
+
+    om = oracle.mesh.perturbed_mesh(nx, nx, JITTER, MESH_SEED)  # same vertices as jittered_rectangle_mesh
+    mean = FixedState.from_primitive(1.0, 0.0, 0.0, 1.0, 1.4)
+    s = oracle.OracleSolver(om, {t: mean for t in ("left", "right", "bottom", "top")}, flux="roe",
+                            limiter="unlimited", gamma=1.4)
+    x, y = s.node_coordinates()
+    rng = np.random.default_rng(FIELD_SEED)
+    rho = fourier_field(x, y, rng, 0.5, 1.5, np)
+    u = fourier_field(x, y, rng, -0.5, 0.5, np)
+    v = fourier_field(x, y, rng, -0.5, 0.5, np)
+    p = fourier_field(x, y, rng, 0.5, 1.5, np)
+    q = oracle.primitive_to_conserved(rho, u, v, p, 1.4)
+    dt = s.time_step(q)
+    q, _ = s.step(q, dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = s.time_step(q)
+        q, _ = s.step(q, dt)
+    return s.mesh.num_elements, steps, time.perf_counter() - t0
+
+
+def cpu_baseline(nx: int, steps: int, processes: int) -> dict:
+    """The CPU oracle (NumPy restatement of the reference) on `processes`
+    spawned workers, each timing `steps` RK3 steps of an nx x nx sample."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(processes) as pool:
+        results = pool.map(_oracle_sample_worker, [(nx, steps)] * processes)
+    k = results[0][0]
+    slowest = max(r[2] for r in results)
+    value = processes * k * NP_NODES * steps / slowest
+    return {"value": value, "unit": "DOF-steps/s", "cores": processes, "kind": "port",
+            "sample": f"{processes} process(es) x {steps} RK3 steps of a {nx}x{nx} sample of the workload "
+                      f"(K={k}, roe/unlimited), NumPy float64 oracle; {slowest:.1f} s"}
+
+
+# ----------------------------------------------------------------- clocks ---
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str):
+        self.bus_id = bus_id.lower()
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                bus = parts[1].lower()
+                if self.bus_id and not (bus.endswith(self.bus_id[-12:]) or self.bus_id.endswith(bus[-12:])):
+                    continue
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[6:10]) if v.strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][3]),
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(float(r[4]) for r in rows)}
+
+
+# -------------------------------------------------------------- GPU timing ---
+def _barrier(world: int) -> None:
+    import torch
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+
+def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: bool = True) -> dict:
+    """Advance the resident state `warmup` + `steps` RK3 steps (device CFL dt,
+    device run-loop control); time the `steps` with CUDA events on the
+    launching stream, and each stage launch separately."""
+    import ctypes as C
+
+    import torch
+
+    from cfd_demo_b200 import _native
+
+    lib, st = solver._lib, solver.native
+    ws = solver._ws
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    ptr = C.byref(st)
+    x0, x1, sg = ws.x0.data_ptr(), ws.x1.data_ptr(), ws.stage.data_ptr()
+
+    def one_step(ev=None):
+        _native.check(lib.cfd_rk3_begin(ptr, sp))
+        for k in (1, 2, 3):
+            if ev is not None:
+                ev[k - 1][0].record(stream)
+            _native.check(lib.cfd_rk3_stage(ptr, x0, x1, sg, k, sp))
+            if ev is not None:
+                ev[k - 1][1].record(stream)
+        _native.check(lib.cfd_rk3_finish(ptr, sp))
+        _native.check(lib.cfd_run_control(ptr, sp))
+
+    for _ in range(warmup):
+        one_step()
+    _barrier(world)
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)] for _ in range(steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for i in range(steps):
+        one_step(evs[i] if stage_events else None)
+    stop.record(stream)
+    _barrier(world)
+    total_ms = start.elapsed_time(stop)
+    stage_ms = [sum(evs[i][k][0].elapsed_time(evs[i][k][1]) for i in range(steps)) for k in range(3)]
+    c = solver._read(ws.control, _native.CfdControl)
+    if c.status != _native.RUN_ACTIVE:
+        raise RuntimeError(f"run-loop status {c.status} during the benchmark")
+    return {"total_ms": total_ms, "stage_ms": stage_ms, "launches_per_step": 6, "time": c.time, "steps_done": c.steps}
+
+
+def l1_density(solver, qa, qb) -> float:
+    """Domain-averaged L1 of rho_a - rho_b by the nodal quadrature."""
+    w = solver.reference.cell_weights
+    jac = np.asarray(solver.geometry.jacobian)
+    diff = np.abs(qa[..., 0] - qb[..., 0])
+    return float(np.einsum("i,ik,k->", w, diff, jac) / np.einsum("i,k->", w, jac))
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def run_ours(args, rank: int, world: int) -> dict | None:
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nx = args.nx
+    steps, warmup = args.steps, args.warmup
+
+    t_setup = time.perf_counter()
+    fp32, q0 = make_workload(nx, "fp32_mixed", dev)
+    fp64 = fp32.with_precision("fp64")
+    setup_s = time.perf_counter() - t_setup
+    k = fp32.mesh.num_elements
+    dof = k * NP_NODES
+
+    results = {}
+    for name, solver in (("fp64", fp64), ("fp32_mixed", fp32)):
+        solver.begin_run(q0, math.inf)
+        if name == "fp32_mixed":
+            props = torch.cuda.get_device_properties(dev)
+            bus = str(getattr(props, "pci_bus_id", "") or "")
+            sampler = ClockSampler(bus)
+            with sampler:
+                r = timed_steps(solver, steps, warmup, world)
+            r["clocks"] = sampler.summary()
+        else:
+            r = timed_steps(solver, steps, warmup, world)
+        r["state"] = solver.download(solver.state_tensor())
+        results[name] = r
+
+    # max over ranks of the timed region
+    tot = {n: results[n]["total_ms"] for n in results}
+    if world > 1:
+        t = torch.tensor([tot["fp32_mixed"], tot["fp64"]], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot = {"fp32_mixed": float(t[0]), "fp64": float(t[1])}
+
+    # end to end through the public API: pinned host state in, host result out
+    host_q0 = q0.cpu().pin_memory()
+    t_k = results["fp32_mixed"]["time"]
+    fp32.run(host_q0, t_k)  # warm (captures the chunk graphs)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    res = fp32.run(host_q0, t_k)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - w0
+    e2e_steps = res.steps
+    e2e_t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_s = float(e2e_t[0])
+
+    if rank != 0:
+        return None
+
+    peak, peak_kind = measured_peak_hbm()
+    out = {}
+    for name, real in (("fp32_mixed", 4), ("fp64", 8)):
+        r = results[name]
+        sb = stage_bytes(real)
+        stage_s = [ms / 1e3 / steps for ms in r["stage_ms"]]
+        achieved = sum(sb) * k / sum(stage_s) / 1e9
+        out[name] = {
+            "value": world * dof * steps / (tot[name] / 1e3),
+            "ms_per_step": tot[name] / steps,
+            "stage_ms": [round(1e3 * s, 4) for s in stage_s],
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_element_step": sum(sb)},
+        }
+    l1 = l1_density(fp32, results["fp32_mixed"]["state"], results["fp64"]["state"])
+    state_bytes = q0.numel() * 8
+    line = {
+        "metric": METRIC,
+        "value": out["fp32_mixed"]["value"],
+        "unit": "DOF-steps/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": out["fp32_mixed"]["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"1M-triangle RK3 microbenchmark: {nx}x{nx} quads x 2 triangles, jitter +-{JITTER}h, "
+                        "8-mode Fourier fields, roe/unlimited, fixed-state boundaries",
+            "elements_per_gpu": k, "np": NP_NODES, "dof_per_gpu": dof, "flux": "roe", "limiter": "unlimited",
+            "precision": "fp32_mixed (f32 state/arithmetic; f64 averages, positivity, reductions)",
+            "dof_definition": "K*Np solution nodes, each with 4 conserved scalars",
+            "step": "one SSP-RK3 step: 3 fused stage kernels + device CFL dt + device run-loop control",
+            "l2": "inputs larger than L2 (state 252 MB f32 / 503 MB f64 per buffer > 126 MB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "setup_s": round(setup_s, 2),
+        },
+        "roofline": out["fp32_mixed"]["roofline"],
+        "stage_ms": out["fp32_mixed"]["stage_ms"],
+        "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms_per_step"],
+                 "stage_ms": out["fp64"]["stage_ms"], "roofline": out["fp64"]["roofline"], "dtype": "f64"},
+        "fp32_over_fp64": out["fp32_mixed"]["value"] / out["fp64"]["value"],
+        "l1_rho_vs_fp64": l1,
+        "e2e": {"value": world * dof * e2e_steps / e2e_s, "unit": "DOF-steps/s",
+                "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": (state_bytes + 104 * e2e_steps) / e2e_steps,
+                "api": "EulerSolver.run(pinned host (Np,K,4) float64 state, t_K) -> RunResult with host state",
+                "steps": e2e_steps, "seconds": e2e_s},
+        "gpu_launches": 6 * steps,
+        "clocks": results["fp32_mixed"]["clocks"],
+    }
+    return line
+
+
+def run_reference(args) -> dict:
+    """The reference arm: the CPU oracle (NumPy restatement of the reference's
+    own algorithm; JAX is not installed) on the host cores."""
+    procs = args.cpu_procs or os.cpu_count() or 1
+    steps = args.steps
+    base = cpu_baseline(args.ref_nx, steps, procs)
+    return {
+        "metric": METRIC, "value": base["value"], "unit": "DOF-steps/s", "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"sample of the 1M-triangle RK3 microbenchmark ({args.ref_nx}x{args.ref_nx} quads x 2), "
+                               "roe/unlimited", "flux": "roe", "limiter": "unlimited"},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "DOF-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ref-nx", type=int, default=48)
+    ap.add_argument("--cpu-procs", type=int, default=0)
+    ap.add_argument("--cpu-baseline-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    # CPU baseline first (spawned workers, before any CUDA context)
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args.ref_nx, args.cpu_baseline_steps, args.cpu_procs or os.cpu_count() or 1)
+
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        torch.distributed.barrier()
+    line = run_ours(args, rank, world)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -72,6 +72,9 @@ _PROTOS = {
     "cfd_integrate": (C.c_int, [_SP, _p, _p, _p]),
     "cfd_check_state": (C.c_int, [_SP, _p, _p, _p]),
     "cfd_rk3_attempt": (C.c_int, [_SP, _p, _p, _p, _p]),
+    "cfd_rk3_begin": (C.c_int, [_SP, _p]),
+    "cfd_rk3_stage": (C.c_int, [_SP, _p, _p, _p, _i32, _p]),
+    "cfd_rk3_finish": (C.c_int, [_SP, _p]),
     "cfd_run_control": (C.c_int, [_SP, _p]),
     "cfd_run_init": (C.c_int, [_SP, _p, _p, _p]),
     "cfd_interface_flux": (C.c_int, [_i32, _i32, _p, _p, _p, _p, _f64, _p, _p]),

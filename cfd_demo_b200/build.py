@@ -39,6 +39,8 @@ def _array(name: str, a: np.ndarray, ctype: str = "double") -> str:
     dims = "".join(f"[{d}]" for d in a.shape)
     if ctype == "int":
         body = ", ".join(str(int(v)) for v in a.ravel())
+    elif ctype == "float":
+        body = ", ".join(repr(float(np.float32(v))) + "f" for v in a.ravel())
     else:
         body = ", ".join(_fmt(v) for v in a.ravel())
     return f"__device__ constexpr {ctype} {name}{dims} = {{{body}}};\n"
@@ -71,6 +73,10 @@ def generate_tables() -> str:
         _array("DR", ref.dr).replace("__device__ constexpr", "__constant__"),
         _array("DS", ref.ds).replace("__device__ constexpr", "__constant__"),
         _array("LIFT", ref.lift).replace("__device__ constexpr", "__constant__"),
+        _array("DR32", ref.dr, "float").replace("__device__ constexpr", "__constant__"),
+        _array("DS32", ref.ds, "float").replace("__device__ constexpr", "__constant__"),
+        _array("LIFT32", ref.lift, "float").replace("__device__ constexpr", "__constant__"),
+        _array("AVG_W", w / w.sum()).replace("__device__ constexpr", "__constant__"),
         _array("FACE_NODES", ref.face_nodes, "int").replace("__device__ constexpr", "__constant__"),
         _array("FACE_W", ref.face_weights[0]).replace("__device__ constexpr", "__constant__"),
         "}}  // namespace cfd::ctab\n",

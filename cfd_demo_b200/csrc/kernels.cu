@@ -59,13 +59,14 @@ __device__ __forceinline__ bool finite_(float x) { return isfinite(x); }
 
 // Face node k of face f, packed 4 bits per entry (tab::FACE_NODES_PACKED).
 constexpr unsigned long long FN_PACK = tab::FACE_NODES_PACKED;
-__device__ __forceinline__ int face_node_rt(int f, int k) { return (int)((FN_PACK >> (4 * (f * NFP + k))) & 15ull); }
 
-// FP32 form: drop the [Dr|Ds] entries that are round-off zeros of the
-// construction (|D| < 1e-13; 65 of 225 per matrix). The FP64 form keeps all.
+// FP32 form: skip the [Dr|Ds] entries that are round-off zeros of the
+// construction (|D| < 1e-13: 65 of 225 per matrix). The FP64 form keeps all.
 template <typename R> __host__ __device__ constexpr bool keep_entry(double v) {
   return sizeof(R) == 8 ? true : (v > 1e-13 || v < -1e-13);
 }
+__device__ __forceinline__ int face_node_rt(int f, int k) { return (int)((FN_PACK >> (4 * (f * NFP + k))) & 15ull); }
+
 
 template <typename R> struct GeoPtr;
 template <> struct GeoPtr<double> {
@@ -175,6 +176,47 @@ __device__ __forceinline__ double pressure_near(double q0, double q1, double q2,
   return (p - bound > margin || p != p) ? p : pressure_x(q0, q1, q2, q3, gm1);
 }
 
+// Constant-bank operator tables in the arithmetic type (warp-uniform index).
+template <typename R> struct tabv;
+template <> struct tabv<double> {
+  static __device__ __forceinline__ double dr(int i, int j) { return ctab::DR[i][j]; }
+  static __device__ __forceinline__ double ds(int i, int j) { return ctab::DS[i][j]; }
+  static __device__ __forceinline__ double lift(int i, int j) { return ctab::LIFT[i][j]; }
+};
+template <> struct tabv<float> {
+  static __device__ __forceinline__ float dr(int i, int j) { return ctab::DR32[i][j]; }
+  static __device__ __forceinline__ float ds(int i, int j) { return ctab::DS32[i][j]; }
+  static __device__ __forceinline__ float lift(int i, int j) { return ctab::LIFT32[i][j]; }
+};
+
+// |u| + c of a node (time_integration.py:39-40). The plain form follows the
+// reference's operation order exactly (divisions, unfused), so the CFL step
+// of a given state is the reference's to the last bit.
+template <typename R>
+__device__ __forceinline__ double wave_speed(R q0, R q1, R q2, R q3, double gamma) {
+  if (sizeof(R) == 8) {
+    const double u = xdiv(q1, q0), v = xdiv(q2, q0);
+    const double p = xmul(gamma - 1.0, xsub(q3, xmul(0.5, xadd(xmul(q1, u), xmul(q2, v)))));
+    return xadd(__dsqrt_rn(xadd(xmul(u, u), xmul(v, v))), __dsqrt_rn(xdiv(xmul(gamma, p), q0)));
+  }
+  const float ir = __frcp_rn((float)q0);
+  const float u = (float)q1 * ir, v = (float)q2 * ir;
+  const float p = (float)(gamma - 1.0) * ((float)q3 - 0.5f * ((float)q1 * u + (float)q2 * v));
+  return (double)(sqrtf(u * u + v * v) + sqrtf((float)gamma * p * ir));
+}
+
+// Exact-order pressure of a node for the positivity test and the minima:
+// the fast form unless it lies within rounding of `bound`.
+template <typename R>
+__device__ __forceinline__ double node_pressure(R q0, R q1, R q2, R q3, double gm1, double bound) {
+  if (sizeof(R) == 8) return pressure_near(q0, q1, q2, q3, gm1, bound);
+  const float ir = __frcp_rn((float)q0);
+  const float k = 0.5f * ((float)q1 * ((float)q1 * ir) + (float)q2 * ((float)q2 * ir));
+  const float p = (float)gm1 * ((float)q3 - k);
+  const float margin = 1e-5f * (fabsf((float)q3) + fabsf(k));
+  return ((double)p - bound > (double)margin || p != p) ? (double)p : pressure_x(q0, q1, q2, q3, gm1);
+}
+
 // Cell average in double, sequential and unfused like NumPy's einsum
 // (limiting.py:209, dg.py:168-171).
 template <typename R>
@@ -260,13 +302,11 @@ __device__ __forceinline__ void element_stats(const R (&q)[NP][4], double gm1, d
 #pragma unroll
   for (int i = 0; i < NP; ++i) {
     const double r = q[i][0], mx = q[i][1], my = q[i][2], en = q[i][3];
-    const double ir = __drcp_rn(r);
-    const double u = mx * ir, v = my * ir;
-    const double p = pressure_near(r, mx, my, en, gm1, 0.0);
+    const double p = node_pressure<R>(q[i][0], q[i][1], q[i][2], q[i][3], gm1, POSITIVITY_FLOOR);
     rmin = fmin(rmin, r);
     pmin = fmin(pmin, p);
     // time_integration.py:39-40: |u| + c
-    const double s = sqrt(u * u + v * v) + sqrt(gamma * p * ir);
+    const double s = wave_speed<R>(q[i][0], q[i][1], q[i][2], q[i][3], gamma);
     lam_nan |= (s != s);
     lam = fmax(lam, s);
 #pragma unroll
@@ -275,67 +315,6 @@ __device__ __forceinline__ void element_stats(const R (&q)[NP][4], double gm1, d
   if (lam_nan) lam = NAN;
 }
 
-
-// ---- volume term: acc = -(Dr Ft + Ds Gt), Ft = rx F + ry G, Gt = sx F + sy G
-// (dg.py:148-151). Fully unrolled: [Dr|Ds] are immediates / constant-bank
-// operands and round-off zeros are skipped at compile time (FP32 form).
-template <typename R>
-__device__ __forceinline__ void volume_unrolled(const R* __restrict__ src, int e, int ld, R gm1, R rx, R ry, R sx, R sy,
-                                                R (&acc)[NP][4]) {
-#pragma unroll
-  for (int j = 0; j < NP; ++j) {
-    R qj[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) qj[c] = src[(c * NP + j) * ld + e];
-    const Prim<R> w = primitive(qj, gm1);
-    R f[4], g[4];
-    cartesian(qj, w, f, g);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const R ft = rx * f[c] + ry * g[c];
-      const R gt = sx * f[c] + sy * g[c];
-#pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        R t = (j == 0) ? R(0) : acc[i][c];
-        if (keep_entry<R>(tab::DR[i][j])) t = fma((R)(-tab::DR[i][j]), ft, t);
-        if (keep_entry<R>(tab::DS[i][j])) t = fma((R)(-tab::DS[i][j]), gt, t);
-        acc[i][c] = t;
-      }
-    }
-  }
-}
-
-// Rolled over j (FP64 form): the 120-register accumulator tile stays resident
-// and the table column is a warp-uniform constant-bank read.
-template <typename R>
-__device__ __forceinline__ void volume_rolled(const R* __restrict__ src, int e, int ld, R gm1, R rx, R ry, R sx, R sy,
-                                              R (&acc)[NP][4]) {
-#pragma unroll
-  for (int i = 0; i < NP; ++i)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[i][c] = R(0);
-#pragma unroll 1
-  for (int j = 0; j < NP; ++j) {
-    R qj[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) qj[c] = src[(c * NP + j) * ld + e];
-    const Prim<R> w = primitive(qj, gm1);
-    R f[4], g[4];
-    cartesian(qj, w, f, g);
-    R ft[4], gt[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      ft[c] = rx * f[c] + ry * g[c];
-      gt[c] = sx * f[c] + sy * g[c];
-    }
-#pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      const R dr = (R)ctab::DR[i][j], ds = (R)ctab::DS[i][j];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[i][c] = fma(-ds, gt[c], fma(-dr, ft[c], acc[i][c]));
-    }
-  }
-}
 
 // One face node of the surface term: exterior state, interface flux, lifted
 // jump, boundary-flux contribution (dg.py:153-164, boundary: dg.py:119-137).
@@ -366,65 +345,6 @@ __device__ __forceinline__ void face_node_flux(const CfdMesh& m, const R* __rest
   if (kind != CFD_FACE_INTERIOR) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) red.b[c] += bw * (double)fhat[c];
-  }
-}
-
-template <typename R, int FLUX>
-__device__ __forceinline__ void surface_unrolled(const CfdMesh& m, const R* __restrict__ src, int e, int ld, R gamma,
-                                                 R (&acc)[NP][4], Red& red) {
-  const R* __restrict__ fg = GeoPtr<R>::face(m);
-  const int finfo = m.face_info[e];
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    const int info = (finfo >> (8 * f)) & 0xff;
-    const int kind = info & 3;
-    const int nf = (info >> 2) & 3;
-    const R nx = fg[(3 * f) * ld + e], ny = fg[(3 * f + 1) * ld + e], fs = fg[(3 * f + 2) * ld + e];
-    const int nb = (kind != CFD_FACE_SLIP_WALL) ? m.neighbor[f * ld + e] : 0;
-    const double hl = (kind != CFD_FACE_INTERIOR) ? m.face_hlen[f * ld + e] : 0.0;
-    const bool same_order = (f == 2) != (nf == 2);
-#pragma unroll
-    for (int k = 0; k < NFP; ++k) {
-      const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);
-      R jump[4];
-      face_node_flux<R, FLUX>(m, src, e, ld, gamma, tab::FACE_NODES[f][k], kind, nb, pn, nx, ny, fs,
-                              tab::FACE_W[k] * hl, jump, red);
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-#pragma unroll
-        for (int i = 0; i < NP; ++i) acc[i][c] = fma((R)tab::LIFT[i][f * NFP + k], jump[c], acc[i][c]);
-    }
-  }
-}
-
-template <typename R, int FLUX>
-__device__ __forceinline__ void surface_rolled(const CfdMesh& m, const R* __restrict__ src, int e, int ld, R gamma,
-                                               R (&acc)[NP][4], Red& red) {
-  const R* __restrict__ fg = GeoPtr<R>::face(m);
-  const int finfo = m.face_info[e];
-#pragma unroll 1
-  for (int f = 0; f < 3; ++f) {
-    const int info = (finfo >> (8 * f)) & 0xff;
-    const int kind = info & 3;
-    const int nf = (info >> 2) & 3;
-    const R nx = fg[(3 * f) * ld + e], ny = fg[(3 * f + 1) * ld + e], fs = fg[(3 * f + 2) * ld + e];
-    const int nb = (kind != CFD_FACE_SLIP_WALL) ? m.neighbor[f * ld + e] : 0;
-    const double hl = (kind != CFD_FACE_INTERIOR) ? m.face_hlen[f * ld + e] : 0.0;
-    const bool same_order = (f == 2) != (nf == 2);
-#pragma unroll 1
-    for (int k = 0; k < NFP; ++k) {
-      const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);
-      R jump[4];
-      face_node_flux<R, FLUX>(m, src, e, ld, gamma, ctab::FACE_NODES[f][k], kind, nb, pn, nx, ny, fs,
-                              ctab::FACE_W[k] * hl, jump, red);
-      const int col = f * NFP + k;
-#pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        const R l = (R)ctab::LIFT[i][col];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[i][c] = fma(l, jump[c], acc[i][c]);
-      }
-    }
   }
 }
 
@@ -464,112 +384,7 @@ __device__ __forceinline__ void select_buffers(const StageParams& P, int par, co
   }
 }
 
-template <typename R, int FLUX, int MODE, int BS>
-__global__ void __launch_bounds__(BS) stage_kernel(const StageParams P) {
-  const CfdMesh& m = P.m;
-  const int ld = m.ld;
-  const int e = blockIdx.x * BS + threadIdx.x;
-  bool live = e < m.num_elements;
-  int inst = 0;
-  if (live && m.instance) inst = m.instance[e];
-  double dt = 0.0;
-  int par = 0;
-  if (live && MODE != MODE_RHS) {
-    const CfdControl* c = P.ctl + inst;
-    live = c->status == CFD_RUN_ACTIVE;
-    dt = c->dt;
-    par = c->parity;
-  }
-  Red red;
-  red.init();
-  if (live) {
-    const R* src_;
-    const R* base_;
-    R* dst_;
-    if (MODE == MODE_RHS) {
-      src_ = (const R*)P.q_in;
-      base_ = nullptr;
-      dst_ = (R*)P.q_out;
-    } else {
-      select_buffers<R>(P, par, src_, base_, dst_);
-    }
-    const R* __restrict__ src = src_;
-    const R* __restrict__ base = base_;
-    R* __restrict__ dst = dst_;
-    const R gamma = (R)P.gamma;
-    const R gm1 = gamma - R(1);
-    const R* __restrict__ mg = GeoPtr<R>::metric(m);
-    const R rx = mg[e], ry = mg[ld + e], sx = mg[2 * ld + e], sy = mg[3 * ld + e];
-
-    R acc[NP][4];
-    if (sizeof(R) == 4) {
-      volume_unrolled<R>(src, e, ld, gm1, rx, ry, sx, sy, acc);
-      surface_unrolled<R, FLUX>(m, src, e, ld, gamma, acc, red);
-    } else {
-      volume_rolled<R>(src, e, ld, gm1, rx, ry, sx, sy, acc);
-      surface_rolled<R, FLUX>(m, src, e, ld, gamma, acc, red);
-    }
-
-    if (MODE == MODE_RHS) {
-#pragma unroll
-      for (int i = 0; i < NP; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) dst[(c * NP + i) * ld + e] = acc[i][c];
-    } else {
-      // ---- SSP-RK3 stage combine (time_integration.py:61-66)
-      const R rdt = (R)dt;
-#pragma unroll
-      for (int i = 0; i < NP; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int idx = (c * NP + i) * ld + e;
-          const R v = src[idx] + rdt * acc[i][c];
-          if (P.stage_idx == 1) acc[i][c] = v;
-          else if (P.stage_idx == 2) acc[i][c] = R(0.75) * base[idx] + R(0.25) * v;
-          else acc[i][c] = base[idx] * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
-        }
-      // ---- cell averages in double (limiting.py:209)
-      double a[4];
-      cell_average<R>(acc, a);
-      const double gm1d = P.gamma - 1.0;
-      const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1d);
-      if (!(a[0] > 0.0) || !(pa > 0.0)) red.fl |= FLAG_BAD_AVERAGE;
-      if (MODE == MODE_UNLIMITED) positivity<R>(acc, a, gm1d);
-#pragma unroll
-      for (int i = 0; i < NP; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) dst[(c * NP + i) * ld + e] = acc[i][c];
-      double rmin, pmin, lam;
-      bool finite;
-      element_stats<R>(acc, gm1d, P.gamma, rmin, pmin, lam, finite);
-      if (!finite) red.fl |= FLAG_NONFINITE;
-      if (MODE == MODE_LIMITED) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) P.avg[c * ld + e] = a[c];
-        P.aux[e] = rmin;
-        P.aux[ld + e] = pmin;
-        if (P.stage_idx == 3) P.aux[2 * ld + e] = lam;
-      } else {
-        red.kr = dkey(rmin);
-        red.kp = dkey(pmin);
-        if (P.stage_idx == 3) {
-          const double d = m.dt_geo[e] / lam;
-          red.kd = dkey(d);
-          if (d != d) red.fl |= FLAG_NAN_DT;
-        }
-      }
-    }
-  }
-  if (MODE == MODE_RHS) {
-    if (live) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-        if (red.b[c] != 0.0) atomicAdd(&P.bflux_out[inst * 4 + c], red.b[c]);
-    }
-  } else {
-    block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
-  }
-}
+#include "stage_pair.cuh"
 
 // ----------------------------------------------------------- limit kernel ---
 struct LimitParams {
@@ -1040,10 +855,10 @@ static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + 
 // Dispatch helpers ------------------------------------------------------------
 template <typename R, int FLUX, int MODE>
 static void launch_stage_bs(const StageParams& p, int bs, cudaStream_t st) {
-  const unsigned g = blocks_for(p.m.num_elements, bs);
-  if (bs == 64) stage_kernel<R, FLUX, MODE, 64><<<g, 64, 0, st>>>(p);
-  else if (bs == 256) stage_kernel<R, FLUX, MODE, 256><<<g, 256, 0, st>>>(p);
-  else stage_kernel<R, FLUX, MODE, 128><<<g, 128, 0, st>>>(p);
+  const unsigned g = blocks_for(p.m.num_elements, bs / 2);  // two threads per element
+  if (bs == 64) stage_pair_kernel<R, FLUX, MODE, 64><<<g, 64, 0, st>>>(p);
+  else if (bs == 256) stage_pair_kernel<R, FLUX, MODE, 256><<<g, 256, 0, st>>>(p);
+  else stage_pair_kernel<R, FLUX, MODE, 128><<<g, 128, 0, st>>>(p);
 }
 template <typename R, int MODE>
 static void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream_t st) {
@@ -1226,15 +1041,30 @@ int cfd_integrate(const CfdSolver* s, const void* q, double* integral, void* str
   return check_launch("cfd_integrate");
 }
 
-int cfd_rk3_attempt(const CfdSolver* s, void* x0, void* x1, void* stage, void* stream) {
+static int attempt_args(const CfdSolver* s, void* x0, void* x1, void* stage) {
   int rc = validate(s);
   if (rc) return rc;
-  if (!x0 || !x1 || !stage || !s->acc || !s->control || !s->report) return fail(CFD_E_ARG, "cfd_rk3_attempt: null pointer");
-  const bool limited = s->limiter != CFD_LIMITER_UNLIMITED;
-  if (limited && (!s->averages || !s->element_aux)) return fail(CFD_E_ARG, "cfd_rk3_attempt: scratch missing");
-  if (x0 == x1 || x0 == stage || x1 == stage) return fail(CFD_E_ARG, "cfd_rk3_attempt: state buffers must be distinct");
+  if (!x0 || !x1 || !stage || !s->acc || !s->control || !s->report) return fail(CFD_E_ARG, "cfd_rk3: null pointer");
+  if (s->limiter != CFD_LIMITER_UNLIMITED && (!s->averages || !s->element_aux))
+    return fail(CFD_E_ARG, "cfd_rk3: averages / element_aux scratch missing");
+  if (x0 == x1 || x0 == stage || x1 == stage) return fail(CFD_E_ARG, "cfd_rk3: state buffers must be distinct");
+  return CFD_OK;
+}
+
+int cfd_rk3_begin(const CfdSolver* s, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!s->acc) return fail(CFD_E_ARG, "cfd_rk3_begin: null pointer");
+  reset_acc(s, (cudaStream_t)stream);
+  return check_launch("cfd_rk3_begin");
+}
+
+int cfd_rk3_stage(const CfdSolver* s, void* x0, void* x1, void* stage, int32_t k, void* stream) {
+  int rc = attempt_args(s, x0, x1, stage);
+  if (rc) return rc;
+  if (k < 1 || k > 3) return fail(CFD_E_ARG, "cfd_rk3_stage: stage must be 1, 2 or 3");
   cudaStream_t st = (cudaStream_t)stream;
-  reset_acc(s, st);
+  const bool limited = s->limiter != CFD_LIMITER_UNLIMITED;
   StageParams p;
   memset(&p, 0, sizeof(p));
   p.m = s->mesh;
@@ -1242,32 +1072,46 @@ int cfd_rk3_attempt(const CfdSolver* s, void* x0, void* x1, void* stage, void* s
   p.x0 = x0;
   p.x1 = x1;
   p.stage = stage;
+  p.stage_idx = k;
   p.gamma = s->gamma;
   p.avg = s->averages;
   p.aux = s->element_aux;
   p.acc = s->acc;
-  LimitParams lp;
-  memset(&lp, 0, sizeof(lp));
-  lp.m = s->mesh;
-  lp.ctl = s->control;
-  lp.x0 = x0;
-  lp.x1 = x1;
-  lp.stage = stage;
-  lp.gamma = s->gamma;
-  lp.avg = s->averages;
-  lp.aux = s->element_aux;
-  lp.acc = s->acc;
-  for (int k = 1; k <= 3; ++k) {
-    p.stage_idx = k;
-    launch_stage(s, p, limited ? MODE_LIMITED : MODE_UNLIMITED, st);
-    if (limited) {
-      lp.stage_idx = k;
-      launch_limit(s, lp, st);
-    }
+  launch_stage(s, p, limited ? MODE_LIMITED : MODE_UNLIMITED, st);
+  if (limited) {
+    LimitParams lp;
+    memset(&lp, 0, sizeof(lp));
+    lp.m = s->mesh;
+    lp.ctl = s->control;
+    lp.x0 = x0;
+    lp.x1 = x1;
+    lp.stage = stage;
+    lp.stage_idx = k;
+    lp.gamma = s->gamma;
+    lp.avg = s->averages;
+    lp.aux = s->element_aux;
+    lp.acc = s->acc;
+    launch_limit(s, lp, st);
   }
+  return check_launch("cfd_rk3_stage");
+}
+
+int cfd_rk3_finish(const CfdSolver* s, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!s->acc || !s->control || !s->report) return fail(CFD_E_ARG, "cfd_rk3_finish: null pointer");
   const int n = s->mesh.num_instances;
-  report_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, s->control, s->report, n, s->cfl);
-  return check_launch("cfd_rk3_attempt");
+  report_kernel<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(s->acc, s->control, s->report, n, s->cfl);
+  return check_launch("cfd_rk3_finish");
+}
+
+int cfd_rk3_attempt(const CfdSolver* s, void* x0, void* x1, void* stage, void* stream) {
+  int rc = attempt_args(s, x0, x1, stage);
+  if (rc) return rc;
+  if ((rc = cfd_rk3_begin(s, stream))) return rc;
+  for (int k = 1; k <= 3; ++k)
+    if ((rc = cfd_rk3_stage(s, x0, x1, stage, k, stream))) return rc;
+  return cfd_rk3_finish(s, stream);
 }
 
 int cfd_run_control(const CfdSolver* s, void* stream) {

@@ -120,7 +120,6 @@ class Workspace:
         self.control = torch.zeros(n * _native.SIZES["CfdControl"], dtype=torch.uint8, device=dev)
         self.small = torch.zeros(max(4 * n, 3 * n, 8), dtype=torch.float64, device=dev)
         self.small_i = torch.zeros(max(n, 8), dtype=torch.int32, device=dev)
-        self.host_q = torch.empty((15, ops.num_elements, 4), dtype=torch.float64, pin_memory=True)
 
 
 class EulerSolver:
@@ -140,13 +139,29 @@ class EulerSolver:
         self.geometry = element_geometry(mesh)
         kind, state = resolve_boundary_conditions(self.connectivity, self.boundary_conditions)
         self._host = host_tables(mesh, self.connectivity, self.geometry, self.reference, kind, state)
-        self.precision = PRECISIONS[config.precision]
+        self._finish_init(device, block_size, graph_chunk)
+
+    def _finish_init(self, device, block_size: int, graph_chunk: int) -> None:
+        self.precision = PRECISIONS[self.config.precision]
         self.operators = DeviceTables([self._host], device, self.precision)
         self._lib = _native.load()
-        self._ws = Workspace(self.operators, self.precision, config.limiter != "unlimited")
+        self._ws = Workspace(self.operators, self.precision, self.config.limiter != "unlimited")
         self._graph_chunk = int(graph_chunk)
         self._graphs: dict = {}
         self._struct = self._make_struct(block_size)
+
+    def with_precision(self, precision: str, **config_changes) -> "EulerSolver":
+        """A solver on the same mesh and boundary conditions with another
+        arithmetic form (and optionally other config fields), reusing the host
+        setup."""
+        import dataclasses
+
+        other = object.__new__(EulerSolver)
+        for name in ("mesh", "boundary_conditions", "reference", "connectivity", "geometry", "_host"):
+            setattr(other, name, getattr(self, name))
+        other.config = dataclasses.replace(self.config, precision=precision, **config_changes)
+        other._finish_init(self.operators.device, self._struct.block_size, self._graph_chunk)
+        return other
 
     # ---- native plumbing ------------------------------------------------------
     def _make_struct(self, block_size: int) -> _native.CfdSolver:
@@ -190,7 +205,7 @@ class EulerSolver:
         if isinstance(q, torch.Tensor):
             if tuple(q.shape) != self.state_shape:
                 raise ValueError(f"Expected a state of shape {self.state_shape}, got {tuple(q.shape)}.")
-            return q.to(device=self.operators.device, dtype=torch.float64).contiguous()
+            return q.to(device=self.operators.device, dtype=torch.float64, non_blocking=q.is_pinned()).contiguous()
         q = np.asarray(q, dtype=np.float64)
         if q.shape != self.state_shape:
             raise ValueError(f"Expected a state of shape {self.state_shape}, got {q.shape}.")

@@ -209,6 +209,14 @@ int cfd_check_state(const CfdSolver* s, const void* q, double* out, void* stream
  */
 int cfd_rk3_attempt(const CfdSolver* s, void* x0, void* x1, void* stage, void* stream);
 
+/* The three parts of cfd_rk3_attempt, for callers that interleave their own
+ * work or timing: begin zeroes the reduction slots; stage k (1, 2, 3) runs
+ * the fused DG stage kernel and, unless the limiter is `unlimited`, the
+ * limiter kernel; finish writes the report. */
+int cfd_rk3_begin(const CfdSolver* s, void* stream);
+int cfd_rk3_stage(const CfdSolver* s, void* x0, void* x1, void* stage, int32_t k, void* stream);
+int cfd_rk3_finish(const CfdSolver* s, void* stream);
+
 /*
  * cfd_run_control: the body of the reference's run loop (solver.py:180-204)
  * after an attempt, per instance: accept (flip parity, advance time, count,
