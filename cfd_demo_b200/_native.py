@@ -17,6 +17,7 @@ CFD_FP64 = 0
 CFD_FP32_MIXED = 1
 FACE_INTERIOR, FACE_SLIP_WALL, FACE_FIXED_STATE = 0, 1, 2
 RUN_ACTIVE, RUN_DONE, RUN_BAD_DT, RUN_REJECTED = 0, 1, -1, -2
+NOALLOC_MAX_ELEMENTS = 16384  # CFD_NOALLOC_MAX_ELEMENTS of include/cfd_b200.h
 
 _p = C.c_void_p
 _i32 = C.c_int32
@@ -77,6 +78,7 @@ _PROTOS = {
     "cfd_rk3_finish": (C.c_int, [_SP, _p]),
     "cfd_run_control": (C.c_int, [_SP, _p]),
     "cfd_run_init": (C.c_int, [_SP, _p, _p, _p]),
+    "cfd_rk3_step_noalloc": (C.c_int, [C.POINTER(CfdMesh), _i32, _i32, _i32, _f64, _f64, _p, _p, _f64, _p, _p]),
     "cfd_interface_flux": (C.c_int, [_i32, _i32, _p, _p, _p, _p, _f64, _p, _p]),
     "cfd_limiter_phi": (C.c_int, [_i32, _i32, _p, _p, _p]),
 }

@@ -1166,3 +1166,96 @@ int cfd_limiter_phi(int32_t limiter, int32_t n, const double* r, double* out, vo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free RK3 step (no counterpart in the reference).
+//
+// For callers that cannot allocate device memory themselves: a foreign-language
+// binding that holds only the pointers it was given and has no CUDA allocator,
+// or an application whose memory pool must not see outside cudaMalloc calls
+// once it has started. All scratch of one step lives in the file-scope array
+// below, which every GPU that loads this library keeps until process exit.
+// ---------------------------------------------------------------------------
+constexpr size_t NOALLOC_LD_MAX = CFD_NOALLOC_MAX_ELEMENTS;  // leading-dimension bound (elements)
+constexpr size_t NOALLOC_STAGE_BYTES = sizeof(double) * 60 * NOALLOC_LD_MAX;  // stage state (f64 or f32)
+constexpr size_t NOALLOC_AVG_BYTES = sizeof(double) * 4 * NOALLOC_LD_MAX;     // stage cell averages
+constexpr size_t NOALLOC_AUX_BYTES = sizeof(double) * 3 * NOALLOC_LD_MAX;     // per-element minima, wave speed
+constexpr size_t NOALLOC_SMALL_BYTES = 1024;  // reduction slots, report, loop state (256-aligned pieces)
+constexpr size_t NOALLOC_BYTES = NOALLOC_STAGE_BYTES + NOALLOC_AVG_BYTES + NOALLOC_AUX_BYTES + NOALLOC_SMALL_BYTES;
+static_assert(3 * sizeof(CfdStageAcc) <= 256 && sizeof(CfdStepReport) <= 256 && sizeof(CfdControl) <= 256,
+              "scratch layout of the allocation-free step");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES];  // device address of g_noalloc_scratch, per device
+}  // namespace
+
+__global__ void noalloc_control_kernel(CfdControl* ctl, double dt) {
+  CfdControl c;
+  memset(&c, 0, sizeof(c));
+  c.final_time = INFINITY;
+  c.dt = dt;
+  c.status = CFD_RUN_ACTIVE;
+  *ctl = c;
+}
+
+__global__ void noalloc_report_kernel(const CfdStepReport* src, CfdStepReport* dst) { *dst = *src; }
+
+extern "C" int cfd_rk3_step_noalloc(const CfdMesh* mesh, int32_t flux, int32_t limiter, int32_t precision, double gamma,
+                                    double cfl, const void* q_in, void* q_out, double dt, CfdStepReport* report,
+                                    void* stream) {
+  if (!mesh || !q_in || !q_out || !report) return fail(CFD_E_ARG, "cfd_rk3_step_noalloc: null pointer");
+  if (q_in == q_out) return fail(CFD_E_ARG, "cfd_rk3_step_noalloc: q_out must not alias q_in");
+  if (mesh->num_instances != 1 || mesh->instance)
+    return fail(CFD_E_ARG, "cfd_rk3_step_noalloc: one mesh instance only");
+  if (mesh->ld < 0 || (size_t)mesh->ld > NOALLOC_LD_MAX) {
+    snprintf(g_err, sizeof(g_err),
+             "cfd_rk3_step_noalloc: mesh leading dimension %d exceeds the static scratch limit of %d elements",
+             (int)mesh->ld, (int)NOALLOC_LD_MAX);
+    return CFD_E_ARG;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("cfd_rk3_step_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(CFD_E_ARG, "cfd_rk3_step_noalloc: device index out of range");
+  // Once per device, with that device current: the device address of the
+  // static array (its host-side name is only a stand-in for it).
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (rc != cudaSuccess || !ptr) {
+      snprintf(g_err, sizeof(g_err), "cfd_rk3_step_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(rc));
+      return CFD_E_CUDA;
+    }
+    g_noalloc_ptr[dev] = (unsigned char*)ptr;
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+  CfdSolver s;
+  memset(&s, 0, sizeof(s));
+  s.mesh = *mesh;
+  s.flux = flux;
+  s.limiter = limiter;
+  s.precision = precision;
+  s.max_rejections = 0;
+  s.gamma = gamma;
+  s.cfl = cfl;
+  void* stage = base;
+  s.averages = (double*)(base + NOALLOC_STAGE_BYTES);
+  s.element_aux = (double*)(base + NOALLOC_STAGE_BYTES + NOALLOC_AVG_BYTES);
+  unsigned char* small = base + NOALLOC_STAGE_BYTES + NOALLOC_AVG_BYTES + NOALLOC_AUX_BYTES;
+  s.acc = (CfdStageAcc*)small;
+  s.report = (CfdStepReport*)(small + 256);
+  s.control = (CfdControl*)(small + 512);
+  s.block_size = 0;
+  int rc = validate(&s);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // The loop state is written fresh on every call; the reduction slots are
+  // zeroed by the attempt itself; averages and aux are written before read.
+  noalloc_control_kernel<<<1, 1, 0, st>>>(s.control, dt);
+  if ((rc = check_launch("cfd_rk3_step_noalloc"))) return rc;
+  if ((rc = cfd_rk3_attempt(&s, const_cast<void*>(q_in), q_out, stage, stream))) return rc;
+  noalloc_report_kernel<<<1, 1, 0, st>>>(s.report, report);
+  return check_launch("cfd_rk3_step_noalloc");
+}

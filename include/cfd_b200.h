@@ -230,6 +230,27 @@ int cfd_run_control(const CfdSolver* s, void* stream);
  * the current state, ...}; minima start from the nodal minima of the state. */
 int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, void* stream);
 
+/*
+ * cfd_rk3_step_noalloc: one SSP-RK3 step of one mesh at the given dt, from
+ * q_in to q_out (device layout, leading dimension mesh->ld), writing the step
+ * report to the device pointer `report`. It has no counterpart in the
+ * reference. It is for callers that cannot allocate device memory: a
+ * foreign-language binding that holds only the buffers it was handed and has
+ * no CUDA allocator of its own, or an application whose memory pool forbids
+ * outside allocations once it runs. Every scratch buffer of the step lives in
+ * a static device array inside this library, sized for meshes with
+ * ld <= CFD_NOALLOC_MAX_ELEMENTS (about 9 MB, held on every GPU that loads the
+ * library until the process exits); larger meshes are refused with CFD_E_ARG.
+ * The call allocates nothing. Its first call on a device looks up the device
+ * address of that array (cudaGetSymbolAddress), so make that first call
+ * before any stream capture. All calls share the one array: calls that
+ * overlap on the GPU (other streams, other host threads) race, and the caller
+ * must serialise them.
+ */
+#define CFD_NOALLOC_MAX_ELEMENTS 16384
+int cfd_rk3_step_noalloc(const CfdMesh* mesh, int32_t flux, int32_t limiter, int32_t precision, double gamma,
+                         double cfl, const void* q_in, void* q_out, double dt, CfdStepReport* report, void* stream);
+
 /* ---- pointwise physics (exercise the device functions of the fused kernels) */
 int cfd_interface_flux(int32_t flux, int32_t n, const double* q_minus, const double* q_plus,
                        const double* nx, const double* ny, double gamma, double* out, void* stream);
