@@ -277,6 +277,15 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     fp32, q0 = make_workload(nx, "fp32_mixed", dev)
     fp64 = fp32.with_precision("fp64")
     setup_s = time.perf_counter() - t_setup
+    from cfd_demo_b200.autotune import autotune
+
+    tuned = {}
+    for name, solver in (("fp32_mixed", fp32), ("fp64", fp64)):
+        if args.variant is None:
+            tuned[name] = autotune(solver, q0)
+        else:
+            solver.set_variant(args.variant)
+            tuned[name] = {"choice": (args.variant, 0), "ms": {}}
     k = fp32.mesh.num_elements
     dof = k * NP_NODES
 
@@ -360,6 +369,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
             "l2": "inputs larger than L2 (state 252 MB f32 / 503 MB f64 per buffer > 126 MB)",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "setup_s": round(setup_s, 2),
+            "stage_kernel": {n: {"choice": list(t["choice"]), "attempt_ms": {k: round(v, 4) for k, v in t["ms"].items()}}
+                             for n, t in tuned.items()},
         },
         "roofline": out["fp32_mixed"]["roofline"],
         "stage_ms": out["fp32_mixed"]["stage_ms"],
@@ -405,6 +416,7 @@ def main() -> None:
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--cpu-baseline-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=None, help="stage-kernel variant (default: autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

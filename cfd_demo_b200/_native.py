@@ -26,7 +26,7 @@ _f64 = C.c_double
 
 class CfdMesh(C.Structure):
     _fields_ = [
-        ("num_elements", _i32), ("ld", _i32), ("num_instances", _i32), ("reserved0", _i32),
+        ("num_elements", _i32), ("ld", _i32), ("num_instances", _i32), ("flags", _i32),
         ("metric", _p), ("face_geo", _p), ("face_hlen", _p), ("dt_geo", _p), ("jacobian", _p), ("cs_coef", _p),
         ("neighbor", _p), ("face_info", _p), ("instance", _p), ("bc_states", _p),
         ("metric32", _p), ("face_geo32", _p), ("cs_coef32", _p),
@@ -53,7 +53,7 @@ class CfdControl(C.Structure):
 class CfdSolver(C.Structure):
     _fields_ = [("mesh", CfdMesh), ("flux", _i32), ("limiter", _i32), ("precision", _i32), ("max_rejections", _i32),
                 ("gamma", _f64), ("cfl", _f64), ("averages", _p), ("element_aux", _p), ("acc", _p),
-                ("report", _p), ("control", _p), ("block_size", _i32), ("reserved1", _i32)]
+                ("report", _p), ("control", _p), ("block_size", _i32), ("variant", _i32)]
 
 
 SIZES = {"CfdMesh": C.sizeof(CfdMesh), "CfdStageAcc": C.sizeof(CfdStageAcc),

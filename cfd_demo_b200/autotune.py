@@ -1,0 +1,67 @@
+"""Autotuner of the stage-kernel shape (elements per block, tile staging).
+
+The fused stage kernel comes in four shapes (CfdSolver.variant):
+  0  tiled, 32 elements (64 threads) per block, state and geometry staged in
+     shared memory, stage base read from global memory in the epilogue
+  1  tiled, 32 elements per block, stage base staged in shared memory too
+  2  register-only pair kernel (block size 64/128/256 threads)
+  3  tiled, 64 elements (128 threads) per block
+`autotune(solver, state)` times one RK3 attempt per candidate on the solver's
+own buffers (an attempt from the same state recomputes the same step, so the
+candidates see identical work), keeps the fastest, and remembers the choice per
+(GPU, precision, flux, limiter, size bucket) for the life of the process.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+from . import _native
+
+CANDIDATES = ((0, 0), (1, 0), (3, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
+_cache: dict = {}
+
+
+def _key(solver) -> tuple:
+    import torch
+
+    name = torch.cuda.get_device_name(solver.operators.device)
+    k = solver.operators.num_elements
+    return (name, solver.config.precision, solver.config.flux, solver.config.limiter, int(math.log2(max(k, 1))))
+
+
+def autotune(solver, state, *, repeats: int = 3, candidates=CANDIDATES, use_cache: bool = True) -> dict:
+    """Pick the fastest stage-kernel shape for `solver` on `state` (any state
+    the solver accepts). Returns {"choice": (variant, block), "ms": {...}}."""
+    import torch
+
+    key = _key(solver)
+    if use_cache and key in _cache:
+        variant, block = _cache[key]["choice"]
+        solver.set_variant(variant)
+        solver.set_block_size(block)
+        return _cache[key]
+    solver.begin_run(state, math.inf)
+    ws, lib = solver._ws, solver._lib
+    stream = torch.cuda.current_stream()
+    times = {}
+    for variant, block in candidates:
+        solver.set_variant(variant)
+        solver.set_block_size(block)
+        ptr = C.byref(solver.native)
+        args = (ws.x0.data_ptr(), ws.x1.data_ptr(), ws.stage.data_ptr(), stream.cuda_stream)
+        _native.check(lib.cfd_rk3_attempt(ptr, *args))  # warm-up (first launch configures the kernel)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(repeats):
+            _native.check(lib.cfd_rk3_attempt(ptr, *args))
+        stop.record(stream)
+        stop.synchronize()
+        times[f"variant{variant}/bs{block}"] = start.elapsed_time(stop) / repeats
+    best = min(candidates, key=lambda vb: times[f"variant{vb[0]}/bs{vb[1]}"])
+    solver.set_variant(best[0])
+    solver.set_block_size(best[1])
+    result = {"choice": best, "ms": times}
+    _cache[key] = result
+    return result

@@ -101,7 +101,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not os.path.exists(tables) or open(tables).read() != text:
         with open(tables, "w") as f:
             f.write(text)
-    inputs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh")))
+    inputs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".inc")))
     inputs.append(os.path.join(INCLUDE, "cfd_b200.h"))
     stamp = LIB + ".sha256"
     digest = _digest(inputs)

@@ -385,6 +385,7 @@ __device__ __forceinline__ void select_buffers(const StageParams& P, int par, co
 }
 
 #include "stage_pair.cuh"
+#include "stage_tile.cuh"
 
 // ----------------------------------------------------------- limit kernel ---
 struct LimitParams {
@@ -412,6 +413,10 @@ __global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
   bool live = e < m.num_elements;
   int inst = 0;
   if (live && m.instance) inst = m.instance[e];
+  if (inst < 0) {  // padding between instances
+    live = false;
+    inst = 0;
+  }
   int par = 0;
   if (live && P.ctl) {
     live = P.ctl[inst].status == CFD_RUN_ACTIVE;
@@ -595,8 +600,9 @@ template <typename R, int BS>
 __global__ void __launch_bounds__(BS) dt_kernel(CfdMesh m, const R* __restrict__ q, CfdStageAcc* acc, double gamma,
                                                  double* minima) {
   const int e = blockIdx.x * BS + threadIdx.x;
-  const bool live = e < m.num_elements;
-  const int inst = (live && m.instance) ? m.instance[e] : 0;
+  const int inst_raw = (e < m.num_elements && m.instance) ? m.instance[e] : 0;
+  const bool live = e < m.num_elements && inst_raw >= 0;
+  const int inst = live ? inst_raw : 0;
   Red red;
   red.init();
   if (live) {
@@ -781,6 +787,7 @@ __global__ void averages_kernel(CfdMesh m, const R* __restrict__ q, double* avg,
   if (e >= m.num_elements) return;
   const int ld = m.ld;
   const int inst = m.instance ? m.instance[e] : 0;
+  if (inst < 0) return;  // padding between instances
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     double s = 0.0;
@@ -846,6 +853,9 @@ static int validate(const CfdSolver* s) {
   if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
   if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
     return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
+  if (s->variant < 0 || s->variant > 3) return fail(CFD_E_ARG, "variant must be 0..3");
+  if (s->variant != 2 && s->mesh.instance && s->mesh.num_instances > 1 && (s->mesh.flags & 1) == 0)
+    return fail(CFD_E_ARG, "tiled stage kernels need instance ranges aligned to 64 elements (CfdMesh.flags bit 0)");
   return CFD_OK;
 }
 
@@ -866,16 +876,42 @@ static void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream
   else if (flux == 1) launch_stage_bs<R, 1, MODE>(p, bs, st);
   else launch_stage_bs<R, 2, MODE>(p, bs, st);
 }
+template <typename R, int FLUX, int MODE, int EPB, bool SB>
+static void launch_tile(const StageParams& p, cudaStream_t st) {
+  using L = TileLayout<R, EPB, SB>;
+  static bool configured = false;  // per instantiation: opt in to > 48 KB of dynamic shared memory
+  if (!configured) {
+    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         L::BYTES);
+    configured = true;
+  }
+  const unsigned g = blocks_for(p.m.num_elements, EPB);
+  stage_tile_kernel<R, FLUX, MODE, EPB, SB><<<g, 2 * EPB, L::BYTES, st>>>(p);
+}
+template <typename R, int FLUX, int MODE>
+static void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_t st) {
+  if (variant == 2) launch_stage_bs<R, FLUX, MODE>(p, bs, st);
+  else if (variant == 1) launch_tile<R, FLUX, MODE, 32, true>(p, st);
+  else if (variant == 3) launch_tile<R, FLUX, MODE, 64, false>(p, st);
+  else launch_tile<R, FLUX, MODE, 32, false>(p, st);
+}
+template <typename R, int MODE>
+static void launch_stage_flux2(const StageParams& p, int flux, int variant, int bs, cudaStream_t st) {
+  if (flux == 0) launch_stage_variant<R, 0, MODE>(p, variant, bs, st);
+  else if (flux == 1) launch_stage_variant<R, 1, MODE>(p, variant, bs, st);
+  else launch_stage_variant<R, 2, MODE>(p, variant, bs, st);
+}
 static void launch_stage(const CfdSolver* s, const StageParams& p, int mode, cudaStream_t st) {
   const int bs = bs_of(s);
+  const int v = s->variant;
   if (s->precision == CFD_FP64) {
-    if (mode == MODE_RHS) launch_stage_flux<double, MODE_RHS>(p, s->flux, bs, st);
-    else if (mode == MODE_LIMITED) launch_stage_flux<double, MODE_LIMITED>(p, s->flux, bs, st);
-    else launch_stage_flux<double, MODE_UNLIMITED>(p, s->flux, bs, st);
+    if (mode == MODE_RHS) launch_stage_flux2<double, MODE_RHS>(p, s->flux, v, bs, st);
+    else if (mode == MODE_LIMITED) launch_stage_flux2<double, MODE_LIMITED>(p, s->flux, v, bs, st);
+    else launch_stage_flux2<double, MODE_UNLIMITED>(p, s->flux, v, bs, st);
   } else {
-    if (mode == MODE_RHS) launch_stage_flux<float, MODE_RHS>(p, s->flux, bs, st);
-    else if (mode == MODE_LIMITED) launch_stage_flux<float, MODE_LIMITED>(p, s->flux, bs, st);
-    else launch_stage_flux<float, MODE_UNLIMITED>(p, s->flux, bs, st);
+    if (mode == MODE_RHS) launch_stage_flux2<float, MODE_RHS>(p, s->flux, v, bs, st);
+    else if (mode == MODE_LIMITED) launch_stage_flux2<float, MODE_LIMITED>(p, s->flux, v, bs, st);
+    else launch_stage_flux2<float, MODE_UNLIMITED>(p, s->flux, v, bs, st);
   }
 }
 template <typename R, int PHI>

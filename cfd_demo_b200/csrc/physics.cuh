@@ -24,10 +24,23 @@ template <typename R> __device__ __forceinline__ R jmin(R a, R b) {
 }
 template <typename R> __device__ __forceinline__ R rcp(R x);
 template <> __device__ __forceinline__ double rcp<double>(double x) { return __drcp_rn(x); }
-template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+// FP32-mixed form: the SFU's approximate reciprocal / square root (PTX
+// rcp.approx.ftz.f32 / sqrt.approx.ftz.f32, about 1 ulp) instead of the
+// correctly rounded sequences; the plain FP64 form keeps IEEE operations.
+template <> __device__ __forceinline__ float rcp<float>(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 template <typename R> __device__ __forceinline__ R sqrt_(R x);
 template <> __device__ __forceinline__ double sqrt_<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float sqrt_<float>(float x) { return sqrtf(x); }
+template <> __device__ __forceinline__ float sqrt_<float>(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+template <typename R> __device__ __forceinline__ R div_(R a, R b) { return a / b; }
+template <> __device__ __forceinline__ float div_<float>(float a, float b) { return a * rcp<float>(b); }
 template <typename R> __device__ __forceinline__ R abs_(R x) { return x < R(0) ? -x : (x == R(0) ? R(0) : x); }
 template <> __device__ __forceinline__ double abs_<double>(double x) { return fabs(x); }
 template <> __device__ __forceinline__ float abs_<float>(float x) { return fabsf(x); }
@@ -178,22 +191,22 @@ __device__ __forceinline__ void hllc(const R qm[4], const R qp[4], const Prim<R>
   const R s_p = jmax(unp + cp, un + c);
   const R mass_m = wm.rho * (s_m - unm);
   const R mass_p = wp.rho * (s_p - unp);
-  const R s_star = (wp.p - wm.p + mass_m * unm - mass_p * unp) / nonzero(mass_m - mass_p);
+  const R s_star = div_(wp.p - wm.p + mass_m * unm - mass_p * unp, nonzero(mass_m - mass_p));
   if (s_m >= R(0)) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] = fm[k];
   } else if (s_star >= R(0)) {
-    const R fac = mass_m / nonzero(s_m - s_star);
+    const R fac = div_(mass_m, nonzero(s_m - s_star));
     const R sh = s_star - unm;
     const R st[4] = {fac, fac * (wm.u + sh * nx), fac * (wm.v + sh * ny),
-                     fac * (qm[3] * wm.inv_rho + sh * (s_star + wm.p / nonzero(mass_m)))};
+                     fac * (qm[3] * wm.inv_rho + sh * (s_star + div_(wm.p, nonzero(mass_m))))};
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] = fm[k] + s_m * (st[k] - qm[k]);
   } else if (s_p > R(0)) {
-    const R fac = mass_p / nonzero(s_p - s_star);
+    const R fac = div_(mass_p, nonzero(s_p - s_star));
     const R sh = s_star - unp;
     const R st[4] = {fac, fac * (wp.u + sh * nx), fac * (wp.v + sh * ny),
-                     fac * (qp[3] * wp.inv_rho + sh * (s_star + wp.p / nonzero(mass_p)))};
+                     fac * (qp[3] * wp.inv_rho + sh * (s_star + div_(wp.p, nonzero(mass_p))))};
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] = fp[k] + s_p * (st[k] - qp[k]);
   } else {

@@ -65,7 +65,7 @@ __device__ __noinline__ void positivity_smem(R* s, const double* a, double gm1) 
 template <typename R, int FLUX, int MODE, int BS>
 __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_pair_kernel(const StageParams P) {
   constexpr int EPB = BS / 2;  // elements per block
-  __shared__ R s_elem[BS / 32][4 * NP];  // one element per warp for the rare positivity repair
+  __shared__ R s_rep[BS / 32][4 * NP];  // one element per warp for the rare positivity repair
   const CfdMesh& m = P.m;
   const int ld = m.ld;
   const int half = threadIdx.x & 1;
@@ -75,6 +75,10 @@ __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_p
   const int e = live ? e_raw : m.num_elements - 1;  // dead lanes still take part in the shuffles
   int inst = 0;
   if (m.instance) inst = m.instance[e];
+  if (inst < 0) {  // padding between instances
+    live = false;
+    inst = 0;
+  }
   double dt = 0.0;
   int par = 0;
   if (MODE != MODE_RHS) {
@@ -204,149 +208,7 @@ __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_p
           else if (P.stage_idx == 2) acc[i][cc] = R(0.75) * base[idx] + R(0.25) * v;
           else acc[i][cc] = base[idx] * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
         }
-      // ---- cell averages in double, NumPy order (sequential, unfused)
-      double a[4];
-      {
-        double s0 = xmul(tab::AVG_W[0], (double)acc[0][0]);
-        double s1 = xmul(tab::AVG_W[0], (double)acc[0][1]);
-#pragma unroll
-        for (int i = 1; i < NP; ++i) {
-          if (sizeof(R) == 8) {  // the reference's order: sequential, unfused
-            s0 = xadd(s0, xmul(tab::AVG_W[i], (double)acc[i][0]));
-            s1 = xadd(s1, xmul(tab::AVG_W[i], (double)acc[i][1]));
-          } else {
-            s0 = fma(tab::AVG_W[i], (double)acc[i][0], s0);
-            s1 = fma(tab::AVG_W[i], (double)acc[i][1], s1);
-          }
-        }
-        const double o0 = shfl_pair(s0), o1 = shfl_pair(s1);
-        a[0] = half ? o0 : s0;
-        a[1] = half ? o1 : s1;
-        a[2] = half ? s0 : o0;
-        a[3] = half ? s1 : o1;
-      }
-      const double gm1d = P.gamma - 1.0;
-      const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1d);
-      const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
-      if (live && half == 0 && (!(a[0] > 0.0) || !(pa > 0.0))) red.fl |= FLAG_BAD_AVERAGE;
-      // ---- node states completed by one exchange per node: minima, wave speed, positivity test
-      const bool want_lam = P.stage_idx == 3;
-      double rmin = INFINITY, pmin = INFINITY, lam = -INFINITY, rmin_nan = INFINITY;
-      bool finite = true, lam_nan = false, need_p = false;
-      // nodes 0..7 are tested by the even lane, 8..14 by the odd lane; one
-      // exchange per round completes the node state on its tester
-#pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        const int ia = r, ib = r + 8 < NP ? r + 8 : NP - 1;
-        const R o0 = shfl_pair(half ? acc[ia][0] : acc[ib][0]);
-        const R o1 = shfl_pair(half ? acc[ia][1] : acc[ib][1]);
-        if (half == 1 && r + 8 >= NP) continue;
-        const R q0 = half ? o0 : acc[ia][0], q1 = half ? o1 : acc[ia][1];
-        const R q2 = half ? acc[ib][0] : o0, q3 = half ? acc[ib][1] : o1;
-        finite &= isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3);
-        rmin = fmin(rmin, (double)q0);
-        rmin_nan = jmin(rmin_nan, (double)q0);
-        const double p = node_pressure<R>(q0, q1, q2, q3, gm1d, eps);
-        pmin = fmin(pmin, p);
-        need_p |= p < eps;
-        if (want_lam) {
-          const double sp = wave_speed<R>(q0, q1, q2, q3, P.gamma);
-          lam_nan |= (sp != sp);
-          lam = fmax(lam, sp);
-        }
-      }
-      // combine the two lanes' partial results
-      {
-        const double o_rmin = shfl_pair(rmin), o_pmin = shfl_pair(pmin), o_lam = shfl_pair(lam);
-        const double o_rnan = shfl_pair(rmin_nan);
-        rmin = fmin(rmin, o_rmin);
-        pmin = fmin(pmin, o_pmin);
-        lam = fmax(lam, o_lam);
-        rmin_nan = (rmin_nan != rmin_nan || o_rnan != o_rnan) ? (double)NAN : fmin(rmin_nan, o_rnan);
-        const unsigned bits = (finite ? 1u : 0u) | (need_p ? 2u : 0u) | (lam_nan ? 4u : 0u);
-        const unsigned ob = __shfl_xor_sync(0xffffffffu, bits, 1);
-        finite = (bits & ob & 1u) != 0;
-        need_p = ((bits | ob) & 2u) != 0;
-        lam_nan = ((bits | ob) & 4u) != 0;
-      }
-      if (lam_nan) lam = NAN;
-      if (MODE == MODE_UNLIMITED) {
-        const bool need = live && (rmin_nan < eps || need_p);
-        unsigned todo = __ballot_sync(0xffffffffu, need);
-        // rare: repair the flagged elements of this warp one at a time on a
-        // shared-memory copy of the element
-        R* s = s_elem[threadIdx.x >> 5];
-        const int lane = threadIdx.x & 31;
-        while (todo) {
-          const int leader = (__ffs(todo) - 1) & ~1;  // even lane of the pair
-          todo &= ~(3u << leader);
-          const bool mine = (lane >> 1) == (leader >> 1);
-          if (mine) {
-#pragma unroll
-            for (int i = 0; i < NP; ++i) {
-              s[c0 * NP + i] = acc[i][0];
-              s[(c0 + 1) * NP + i] = acc[i][1];
-            }
-          }
-          __syncwarp();
-          if (lane == leader) {
-            positivity_smem<R>(s, a, gm1d);
-            rmin = INFINITY;
-            pmin = INFINITY;
-            lam = -INFINITY;
-            lam_nan = false;
-            finite = true;
-#pragma unroll 1
-            for (int i = 0; i < NP; ++i) {
-              const R q0 = s[i], q1 = s[NP + i], q2 = s[2 * NP + i], q3 = s[3 * NP + i];
-              finite &= isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3);
-              rmin = fmin(rmin, (double)q0);
-              pmin = fmin(pmin, node_pressure<R>(q0, q1, q2, q3, gm1d, eps));
-              const double sp = wave_speed<R>(q0, q1, q2, q3, P.gamma);
-              lam_nan |= (sp != sp);
-              lam = fmax(lam, sp);
-            }
-            if (lam_nan) lam = NAN;
-          }
-          __syncwarp();
-          if (mine) {
-#pragma unroll
-            for (int i = 0; i < NP; ++i) {
-              acc[i][0] = s[c0 * NP + i];
-              acc[i][1] = s[(c0 + 1) * NP + i];
-            }
-          }
-          __syncwarp();
-        }
-      }
-      if (live) {
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-          dst[(c0 * NP + i) * ld + e] = acc[i][0];
-          dst[((c0 + 1) * NP + i) * ld + e] = acc[i][1];
-        }
-        if (MODE == MODE_LIMITED) {
-          P.avg[c0 * ld + e] = half ? a[2] : a[0];
-          P.avg[(c0 + 1) * ld + e] = half ? a[3] : a[1];
-          if (half == 0) {
-            P.aux[e] = rmin;
-            P.aux[ld + e] = pmin;
-            if (want_lam) P.aux[2 * ld + e] = lam;
-          }
-        }
-        if (half == 0) {
-          if (!finite) red.fl |= FLAG_NONFINITE;
-          if (MODE == MODE_UNLIMITED) {
-            red.kr = dkey(rmin);
-            red.kp = dkey(pmin);
-            if (want_lam) {
-              const double d = m.dt_geo[e] / lam;
-              red.kd = dkey(d);
-              if (d != d) red.fl |= FLAG_NAN_DT;
-            }
-          }
-        }
-      }
+#include "stage_epilogue.inc"
     }
   }
   if (!live) red.init();

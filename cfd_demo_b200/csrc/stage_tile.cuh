@@ -1,0 +1,279 @@
+// stage_tile.cuh — the fused DG stage kernel with shared-memory element tiles.
+//
+// Same arithmetic as stage_pair_kernel (two threads per element, the even lane
+// owning {rho, rho u}, the odd lane {rho v, E}), but every block first stages
+// its EPB elements into shared memory with asynchronous copies so that the
+// long-latency global loads are all in flight at once instead of trickling
+// through the dependent arithmetic:
+//   group A  own state rows [60][EPB] and geometry rows (16-byte cp.async)
+//   group B  the neighbours' face traces (4/8-byte cp.async, one per value)
+//            and, from stage 2 on, the stage base rows; these complete while
+//            the volume term runs from shared memory
+// then the surface rounds, the RK combine and the epilogue read shared memory
+// and only the stage result is stored to global memory (coalesced).
+// Blocks are instance-uniform: several meshes are laid out with every
+// instance starting at a multiple of 64 elements (operators.py).
+#pragma once
+// Included by kernels.cu inside namespace cfd.
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_small(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Shared-memory layout of one block (all offsets in elements of R, 16-byte aligned).
+template <typename R, int EPB, bool STAGE_BASE>
+struct TileLayout {
+  // row stride of the [60][.] state tiles: 30 rows apart (the two lanes'
+  // variables) must fall 16 banks apart, and rows must stay 16-byte aligned
+  static constexpr int S = sizeof(R) == 4 ? EPB + 8 : EPB + 4;
+  static constexpr int OWN = 0;
+  static constexpr int BASE = OWN + 60 * S;
+  static constexpr int NBR = BASE + (STAGE_BASE ? 60 * S : 0);  // [8 rounds][4 vars][EPB][2 lanes]
+  static constexpr int GEO = NBR + 64 * EPB;                      // [13][S]: rx ry sx sy, (nx ny fs) x 3
+  static constexpr int INT_BYTES_OFF = (GEO + 13 * S) * (int)sizeof(R);  // int rows [4][EPB]
+  static constexpr int BYTES = INT_BYTES_OFF + 4 * EPB * 4;
+};
+
+template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE>
+__global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * EPB))
+    stage_tile_kernel(const StageParams P) {
+  constexpr int BS = 2 * EPB;
+  using L = TileLayout<R, EPB, STAGE_BASE>;
+  constexpr int S = L::S;
+  constexpr int VEC = 16 / (int)sizeof(R);  // elements per 16-byte chunk
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* t_own = reinterpret_cast<R*>(smem_raw) + L::OWN;
+  R* t_base = reinterpret_cast<R*>(smem_raw) + L::BASE;
+  R* t_nbr = reinterpret_cast<R*>(smem_raw) + L::NBR;
+  R* t_geo = reinterpret_cast<R*>(smem_raw) + L::GEO;
+  int* t_int = reinterpret_cast<int*>(smem_raw + L::INT_BYTES_OFF);
+  __shared__ R s_rep[BS / 32][4 * NP];  // one element per warp for the rare positivity repair
+
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int K = m.num_elements;
+  const int tid = threadIdx.x;
+  const int half = tid & 1;
+  const int slot = tid >> 1;
+  const int e0 = blockIdx.x * EPB;
+  const int e = e0 + slot;
+  // block-uniform instance and loop state
+  const int inst_raw = m.instance ? m.instance[e0] : 0;
+  bool block_live = inst_raw >= 0;  // a block of padding between instances does nothing
+  const int inst = block_live ? inst_raw : 0;
+  double dt = 0.0;
+  int par = 0;
+  if (MODE != MODE_RHS && block_live) {
+    const CfdControl* c = P.ctl + inst;
+    block_live = c->status == CFD_RUN_ACTIVE;
+    dt = c->dt;
+    par = c->parity;
+  }
+  const bool live = block_live && e < K && (m.instance == nullptr || m.instance[e] == inst);
+  Red red;
+  red.init();
+
+  if (block_live) {
+    const R* src_;
+    const R* base_;
+    R* dst_;
+    if (MODE == MODE_RHS) {
+      src_ = (const R*)P.q_in;
+      base_ = nullptr;
+      dst_ = (R*)P.q_out;
+    } else {
+      select_buffers<R>(P, par, src_, base_, dst_);
+    }
+    const R* __restrict__ src = src_;
+    const R* __restrict__ base = base_;
+    R* __restrict__ dst = dst_;
+    const bool has_base = MODE != MODE_RHS && P.stage_idx >= 2;
+
+    // ---- group A: own state rows and geometry rows
+    {
+      constexpr int CPR = EPB / VEC;  // chunks per row
+      for (int ch = tid; ch < 60 * CPR; ch += BS) {
+        const int row = ch / CPR, col = (ch - row * CPR) * VEC;
+        cp_async16(&t_own[row * S + col], src + (size_t)row * ld + e0 + col);
+      }
+      const R* mg = GeoPtr<R>::metric(m);
+      const R* fg = GeoPtr<R>::face(m);
+      for (int ch = tid; ch < 13 * CPR; ch += BS) {
+        const int row = ch / CPR, col = (ch - row * CPR) * VEC;
+        const R* g = row < 4 ? mg + (size_t)row * ld : fg + (size_t)(row - 4) * ld;
+        cp_async16(&t_geo[row * S + col], g + e0 + col);
+      }
+      constexpr int ICPR = EPB / 4;
+      for (int ch = tid; ch < 4 * ICPR; ch += BS) {
+        const int row = ch / ICPR, col = (ch - row * ICPR) * 4;
+        const int* g = row == 0 ? m.face_info : m.neighbor + (size_t)(row - 1) * ld;
+        cp_async16(&t_int[row * EPB + col], g + e0 + col);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+    }
+    // ---- group B: neighbour face traces (this lane's two variables) and the base rows
+    const int finfo = t_int[slot];
+    if (live) {
+#pragma unroll
+      for (int sl = 0; sl < 3 * NFP; ++sl) {
+        const int f = sl / NFP, k = sl % NFP;
+        const int info = (finfo >> (8 * f)) & 0xff;
+        if ((info & 3) != CFD_FACE_INTERIOR) continue;
+        const int nf = (info >> 2) & 3;
+        const int nb = t_int[(1 + f) * EPB + slot];
+        const bool same_order = (f == 2) != (nf == 2);
+        const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int c = 2 * half + cc;
+          cp_async_small<sizeof(R)>(&t_nbr[(((sl >> 1) * 4 + c) * EPB + slot) * 2 + (sl & 1)],
+                                    src + (size_t)(c * NP + pn) * ld + nb);
+        }
+      }
+    }
+    if (STAGE_BASE && has_base) {
+      constexpr int CPR = EPB / VEC;
+      for (int ch = tid; ch < 60 * CPR; ch += BS) {
+        const int row = ch / CPR, col = (ch - row * CPR) * VEC;
+        cp_async16(&t_base[row * S + col], base + (size_t)row * ld + e0 + col);
+      }
+    }
+    cp_async_commit();
+
+    const R gamma = (R)P.gamma;
+    const R gm1 = gamma - R(1);
+    const int c0 = 2 * half;
+    const R rx = t_geo[0 * S + slot], ry = t_geo[1 * S + slot], sx = t_geo[2 * S + slot], sy = t_geo[3 * S + slot];
+    R acc[NP][2];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) acc[i][0] = acc[i][1] = R(0);
+
+    // ---- volume term from the own tile (dg.py:148-151)
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      R q[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) q[c] = t_own[(c * NP + j) * S + slot];
+      const Prim<R> w = primitive(q, gm1);
+      const R ep = q[3] + w.p;
+      const R fa = half ? q[2] * w.u : q[1];
+      const R fb = half ? ep * w.u : q[1] * w.u + w.p;
+      const R ga = half ? q[2] * w.v + w.p : q[2];
+      const R gb = half ? ep * w.v : q[1] * w.v;
+      const R fta = rx * fa + ry * ga, ftb = rx * fb + ry * gb;
+      const R gta = sx * fa + sy * ga, gtb = sx * fb + sy * gb;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        if (keep_entry<R>(tab::DR[i][j])) {
+          acc[i][0] = fma((R)(-tab::DR[i][j]), fta, acc[i][0]);
+          acc[i][1] = fma((R)(-tab::DR[i][j]), ftb, acc[i][1]);
+        }
+        if (keep_entry<R>(tab::DS[i][j])) {
+          acc[i][0] = fma((R)(-tab::DS[i][j]), gta, acc[i][0]);
+          acc[i][1] = fma((R)(-tab::DS[i][j]), gtb, acc[i][1]);
+        }
+      }
+    }
+
+    cp_async_wait<0>();
+    __syncthreads();
+
+    // ---- surface term (dg.py:153-164): 8 rounds, the lanes take nodes 2r and 2r+1
+#pragma unroll 1
+    for (int r = 0; r < 8; ++r) {
+      const int sl = 2 * r + half;
+      R jump[4] = {R(0), R(0), R(0), R(0)};
+      if (sl < 3 * NFP) {
+        const int f = sl / NFP, k = sl - NFP * f;
+        const int kind = (finfo >> (8 * f)) & 3;
+        const R nx = t_geo[(4 + 3 * f) * S + slot], ny = t_geo[(5 + 3 * f) * S + slot];
+        const R fs = t_geo[(6 + 3 * f) * S + slot];
+        const int n = face_node_rt(f, k);
+        R qm[4], qp[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) qm[c] = t_own[(c * NP + n) * S + slot];
+        if (kind == CFD_FACE_INTERIOR) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) qp[c] = t_nbr[((r * 4 + c) * EPB + slot) * 2 + half];
+        } else if (kind == CFD_FACE_SLIP_WALL) {  // dg.py:119-126
+          const R mn = qm[1] * nx + qm[2] * ny;
+          qp[0] = qm[0];
+          qp[1] = qm[1] - R(2) * mn * nx;
+          qp[2] = qm[2] - R(2) * mn * ny;
+          qp[3] = qm[3];
+        } else {
+          const int row = t_int[(1 + f) * EPB + slot];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
+        }
+        R fhat[4], fm[4];
+        interface_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) jump[c] = fs * (fm[c] - fhat[c]);
+        if (kind != CFD_FACE_INTERIOR) {
+          const double bw = ctab::FACE_W[k] * m.face_hlen[(size_t)f * ld + e];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) red.b[c] += bw * (double)fhat[c];
+        }
+      }
+      const R s0 = shfl_pair(half ? jump[0] : jump[2]);
+      const R s1 = shfl_pair(half ? jump[1] : jump[3]);
+      const R ja0 = half ? s0 : jump[0], ja1 = half ? s1 : jump[1];
+      const R jb0 = half ? jump[2] : s0, jb1 = half ? jump[3] : s1;
+      const int col = 2 * r;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const R la = tabv<R>::lift(i, col);
+        const R lb = col + 1 < 3 * NFP ? tabv<R>::lift(i, col + 1) : R(0);
+        acc[i][0] = fma(lb, jb0, fma(la, ja0, acc[i][0]));
+        acc[i][1] = fma(lb, jb1, fma(la, ja1, acc[i][1]));
+      }
+    }
+
+    if (MODE == MODE_RHS) {
+      if (live) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          dst[(size_t)(c0 * NP + i) * ld + e] = acc[i][0];
+          dst[(size_t)((c0 + 1) * NP + i) * ld + e] = acc[i][1];
+        }
+      }
+    } else {
+      // ---- SSP-RK3 stage combine (time_integration.py:61-66)
+      const R rdt = (R)dt;
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int row = (c0 + cc) * NP + i;
+          const R v = t_own[row * S + slot] + rdt * acc[i][cc];
+          const R b = !has_base ? R(0) : (STAGE_BASE ? t_base[row * S + slot] : base[(size_t)row * ld + e]);
+          if (P.stage_idx == 1) acc[i][cc] = v;
+          else if (P.stage_idx == 2) acc[i][cc] = R(0.75) * b + R(0.25) * v;
+          else acc[i][cc] = b * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
+        }
+#include "stage_epilogue.inc"
+    }
+  }
+  if (!live) red.init();
+  if (MODE == MODE_RHS) {
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (red.b[c] != 0.0) atomicAdd(&P.bflux_out[inst * 4 + c], red.b[c]);
+    }
+  } else {
+    block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
+  }
+}

@@ -180,8 +180,13 @@ class DeviceTables:
 
         self.device = torch.device(device)
         sizes = [p.num_elements for p in parts]
-        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
-        k = int(self.offsets[-1])
+        # several instances: every instance starts at a multiple of LD_ALIGN
+        # elements (padding elements carry instance -1), so that the tiled
+        # kernels' blocks never straddle two instances
+        spans = sizes if len(parts) == 1 else [padded_ld(n) for n in sizes]
+        self.offsets = np.concatenate([[0], np.cumsum(spans)]).astype(np.int64)
+        self.sizes = np.asarray(sizes, dtype=np.int64)
+        k = int(self.offsets[-1]) if len(parts) == 1 else int(self.offsets[-2] + sizes[-1])
         ld = padded_ld(k)
         self.num_elements, self.ld, self.num_instances = k, ld, len(parts)
         bc_off = np.concatenate([[0], np.cumsum([len(p.bc_states) for p in parts])]).astype(np.int64)
@@ -197,7 +202,7 @@ class DeviceTables:
         dt_geo, jac = cat("dt_geo", 1)[0], cat("jacobian", 1)[0]
         nbr = np.zeros((3, ld), dtype=np.int32)
         info = np.zeros(ld, dtype=np.int32)
-        inst = np.zeros(ld, dtype=np.int32)
+        inst = np.full(ld, -1, dtype=np.int32)
         for i, (p, o) in enumerate(zip(parts, self.offsets[:-1])):
             kinds = np.stack([(p.face_info >> (8 * f)) & 3 for f in range(3)])
             local = p.neighbor.astype(np.int64)
@@ -222,6 +227,6 @@ class DeviceTables:
             self.metric32 = self.face_geo32 = self.cs_coef32 = None
         ptr = lambda x: None if x is None else x.data_ptr()  # noqa: E731
         self.struct = _native.CfdMesh(
-            k, ld, len(parts), 0, ptr(self.metric), ptr(self.face_geo), ptr(self.face_hlen), ptr(self.dt_geo),
+            k, ld, len(parts), 1 if len(parts) > 1 else 0, ptr(self.metric), ptr(self.face_geo), ptr(self.face_hlen), ptr(self.dt_geo),
             ptr(self.jacobian), ptr(self.cs_coef), ptr(self.neighbor), ptr(self.face_info), ptr(self.instance),
             ptr(self.bc_states), ptr(self.metric32), ptr(self.face_geo32), ptr(self.cs_coef32))

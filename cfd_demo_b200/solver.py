@@ -126,7 +126,7 @@ class EulerSolver:
     """Degree-four nodal DG solver for the 2D Euler equations on a B200."""
 
     def __init__(self, mesh: TriangleMesh, boundary_conditions: Mapping[str, BoundaryCondition], config: SolverConfig,
-                 *, device="cuda", block_size: int = 0, graph_chunk: int = 32) -> None:
+                 *, device="cuda", block_size: int = 0, graph_chunk: int = 32, variant: int = 0) -> None:
         import torch
 
         if not torch.cuda.is_available():
@@ -139,9 +139,9 @@ class EulerSolver:
         self.geometry = element_geometry(mesh)
         kind, state = resolve_boundary_conditions(self.connectivity, self.boundary_conditions)
         self._host = host_tables(mesh, self.connectivity, self.geometry, self.reference, kind, state)
-        self._finish_init(device, block_size, graph_chunk)
+        self._finish_init(device, block_size, graph_chunk, variant)
 
-    def _finish_init(self, device, block_size: int, graph_chunk: int) -> None:
+    def _finish_init(self, device, block_size: int, graph_chunk: int, variant: int = 0) -> None:
         self.precision = PRECISIONS[self.config.precision]
         self.operators = DeviceTables([self._host], device, self.precision)
         self._lib = _native.load()
@@ -149,6 +149,7 @@ class EulerSolver:
         self._graph_chunk = int(graph_chunk)
         self._graphs: dict = {}
         self._struct = self._make_struct(block_size)
+        self._struct.variant = int(variant)
 
     def with_precision(self, precision: str, **config_changes) -> "EulerSolver":
         """A solver on the same mesh and boundary conditions with another
@@ -160,7 +161,7 @@ class EulerSolver:
         for name in ("mesh", "boundary_conditions", "reference", "connectivity", "geometry", "_host"):
             setattr(other, name, getattr(self, name))
         other.config = dataclasses.replace(self.config, precision=precision, **config_changes)
-        other._finish_init(self.operators.device, self._struct.block_size, self._graph_chunk)
+        other._finish_init(self.operators.device, self._struct.block_size, self._graph_chunk, self._struct.variant)
         return other
 
     # ---- native plumbing ------------------------------------------------------
@@ -189,6 +190,11 @@ class EulerSolver:
 
     def set_block_size(self, block_size: int) -> None:
         self._struct.block_size = int(block_size)
+        self._graphs.clear()
+
+    def set_variant(self, variant: int) -> None:
+        """Select the stage-kernel variant (see CfdSolver.variant)."""
+        self._struct.variant = int(variant)
         self._graphs.clear()
 
     @property

@@ -91,7 +91,9 @@ typedef struct CfdMesh {
     int32_t num_elements;  /* K: elements of all instances */
     int32_t ld;            /* leading dimension, >= num_elements */
     int32_t num_instances; /* >= 1 */
-    int32_t reserved0;
+    int32_t flags;         /* bit 0: every instance starts at a multiple of 64 elements
+                              (padding elements have instance -1); required by the tiled
+                              stage kernels when num_instances > 1 */
     const double* metric;    /* [4][ld]  rx, ry, sx, sy */
     const double* face_geo;  /* [9][ld]  nx_f, ny_f, Fscale_f (= sJ/J) for f = 0,1,2 */
     const double* face_hlen; /* [3][ld]  half edge length (boundary-flux weights) */
@@ -162,8 +164,9 @@ typedef struct CfdSolver {
     CfdStageAcc* acc;      /* [num_instances][3] */
     CfdStepReport* report; /* [num_instances] */
     CfdControl* control;   /* [num_instances] */
-    int32_t block_size;    /* threads per block of the element kernels (64, 128, 256); 0 = default */
-    int32_t reserved1;
+    int32_t block_size;    /* threads per block of the pair stage kernel (64, 128, 256); 0 = default */
+    int32_t variant;       /* stage kernel: 0 tiled (default), 1 tiled + staged base rows,
+                              2 register-only pair kernel, 3 tiled with 64 elements per block */
 } CfdSolver;
 
 /* ---- library ------------------------------------------------------------- */

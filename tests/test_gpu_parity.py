@@ -42,9 +42,10 @@ def test_phi_bit_exact():
 
 @pytest.mark.parametrize("prefix", case_prefixes(load("rhs")))
 @pytest.mark.parametrize("flux", FLUXES)
-def test_rhs_matches_reference(prefix, flux):
+@pytest.mark.parametrize("variant", [0, 2, 3])
+def test_rhs_matches_reference(prefix, flux, variant):
     g = load("rhs")
-    s = make_solver(g, prefix, flux=flux)
+    s = make_solver(g, prefix, flux=flux, variant=variant)
     rhs, bflux = s.rhs(g[f"{prefix}/q"])
     ref = g[f"{prefix}/rhs/{flux}"]
     if prefix == "freestream":
@@ -91,9 +92,10 @@ def test_positivity_floor_is_met_exactly():
 
 @pytest.mark.parametrize("flux", FLUXES)
 @pytest.mark.parametrize("limiter", LIMITERS)
-def test_step_matches_reference(flux, limiter):
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_step_matches_reference(flux, limiter, variant):
     g = load("step")
-    s = make_solver(g, "mesh", flux=flux, limiter=limiter)
+    s = make_solver(g, "mesh", flux=flux, limiter=limiter, variant=variant)
     key = f"{flux}/{limiter}"
     assert s.time_step(g["q"]) == pytest.approx(float(g[f"{key}/dt"]), rel=1e-13)
     qn, rep = s.step(g["q"], float(g[f"{key}/dt"]))
@@ -204,3 +206,17 @@ def test_config0_sod_run(report):
     assert res.min_pressure >= 1e-13 * (1.0 - 1e-9)
     defect = case.solver.integrate(res.state) - case.solver.integrate(case.initial_state) + res.boundary_flux_integral
     assert np.abs(defect).max() <= 1e-12
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_fp32_mixed_step_tracks_fp64(variant):
+    """The FP32-mixed form against the plain form on the step fixture: one RK3
+    step agrees to FP32 accuracy (1e-5 of each variable's scale)."""
+    g = load("step")
+    s64 = make_solver(g, "mesh", flux="roe", limiter="unlimited")
+    s32 = make_solver(g, "mesh", flux="roe", limiter="unlimited", precision="fp32_mixed", variant=variant)
+    dt = float(g["roe/unlimited/dt"])
+    q64, r64 = s64.step(g["q"], dt)
+    q32, r32 = s32.step(g["q"], dt)
+    assert rel_err(q32, q64) <= 1e-5
+    assert r32.admissible and r64.admissible
