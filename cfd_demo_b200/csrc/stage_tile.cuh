@@ -189,8 +189,10 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
     cp_async_wait<0>();
     __syncthreads();
 
-    // ---- surface term (dg.py:153-164): 8 rounds, the lanes take nodes 2r and 2r+1
-#pragma unroll 1
+    // ---- surface term (dg.py:153-164): 8 rounds, the lanes take nodes 2r and 2r+1;
+    // unrolled in the FP32 form so the LIFT columns are compile-time operands
+    // (the FP64 form keeps the loop rolled: fewer live registers)
+#pragma unroll(sizeof(R) == 4 ? 8 : 1)
     for (int r = 0; r < 8; ++r) {
       const int sl = 2 * r + half;
       R jump[4] = {R(0), R(0), R(0), R(0)};
@@ -234,10 +236,15 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
       const int col = 2 * r;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
-        const R la = tabv<R>::lift(i, col);
-        const R lb = col + 1 < 3 * NFP ? tabv<R>::lift(i, col + 1) : R(0);
-        acc[i][0] = fma(lb, jb0, fma(la, ja0, acc[i][0]));
-        acc[i][1] = fma(lb, jb1, fma(la, ja1, acc[i][1]));
+        const R la = sizeof(R) == 4 ? (R)tab::LIFT[i][col] : tabv<R>::lift(i, col);
+        acc[i][0] = fma(la, ja0, acc[i][0]);
+        acc[i][1] = fma(la, ja1, acc[i][1]);
+        if (col + 1 < 3 * NFP) {
+          const int c1 = col + 1 < 3 * NFP ? col + 1 : col;
+          const R lb = sizeof(R) == 4 ? (R)tab::LIFT[i][c1] : tabv<R>::lift(i, c1);
+          acc[i][0] = fma(lb, jb0, acc[i][0]);
+          acc[i][1] = fma(lb, jb1, acc[i][1]);
+        }
       }
     }
 
