@@ -33,6 +33,9 @@ constexpr int NP = 15;
 constexpr int NFP = 5;
 constexpr double NEIGHBOR_FACTOR = 1.5;      // limiting.py:22
 constexpr double DETECTION_TOLERANCE = 1e-10; // limiting.py:24
+// FP32-mixed form: the troubled-cell test compares with ~100 single-precision
+// ulps of the average (1e-10 lies far below the state's own round-off there)
+constexpr double DETECTION_TOLERANCE_FP32 = 1e-5;
 constexpr double POSITIVITY_FLOOR = 1e-13;    // limiting.py:28
 constexpr int BISECTION_STEPS = 60;           // limiting.py:29
 
@@ -199,10 +202,15 @@ __device__ __forceinline__ double wave_speed(R q0, R q1, R q2, R q3, double gamm
     const double p = xmul(gamma - 1.0, xsub(q3, xmul(0.5, xadd(xmul(q1, u), xmul(q2, v)))));
     return xadd(__dsqrt_rn(xadd(xmul(u, u), xmul(v, v))), __dsqrt_rn(xdiv(xmul(gamma, p), q0)));
   }
-  const float ir = __frcp_rn((float)q0);
+  // FP32 form: single precision, except that a pressure lost to cancellation
+  // (near vacuum) is recovered in double before the sound speed is taken
+  const float ir = rcp<float>((float)q0);
   const float u = (float)q1 * ir, v = (float)q2 * ir;
-  const float p = (float)(gamma - 1.0) * ((float)q3 - 0.5f * ((float)q1 * u + (float)q2 * v));
-  return (double)(sqrtf(u * u + v * v) + sqrtf((float)gamma * p * ir));
+  const float kin = 0.5f * ((float)q1 * u + (float)q2 * v);
+  float p = (float)(gamma - 1.0) * ((float)q3 - kin);
+  if (!(p > 1e-4f * (fabsf((float)q3) + kin)))
+    p = (float)pressure_x((double)q0, (double)q1, (double)q2, (double)q3, gamma - 1.0);
+  return (double)(sqrt_<float>(u * u + v * v) + sqrt_<float>((float)gamma * p * ir));
 }
 
 // Exact-order pressure of a node for the positivity test and the minima:
@@ -215,6 +223,17 @@ __device__ __forceinline__ double node_pressure(R q0, R q1, R q2, R q3, double g
   const float p = (float)gm1 * ((float)q3 - k);
   const float margin = 1e-5f * (fabsf((float)q3) + fabsf(k));
   return ((double)p - bound > (double)margin || p != p) ? (double)p : pressure_x(q0, q1, q2, q3, gm1);
+}
+
+// Pressure target of the positivity limiter: the reference's eps
+// (limiting.py:173-176) in the plain form; in the FP32-mixed form eps plus a
+// margin covering the rounding of the repaired state to single precision
+// (|dp| <= ~2e-7 (gamma-1) |E|), capped at half the average pressure so that
+// the average itself stays admissible.
+template <typename R>
+__device__ __forceinline__ double pressure_target(double eps, double pa, double e_avg, double gm1) {
+  if (sizeof(R) == 8) return eps;
+  return eps + jmin(2e-6 * gm1 * fabs(e_avg), 0.5 * pa);
 }
 
 // Cell average in double, sequential and unfused like NumPy's einsum
@@ -237,6 +256,7 @@ template <typename R>
 __device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], double gm1) {
   const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
   const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+  const double pt = pressure_target<R>(eps, pa, a[3], gm1);
   double rmin = (double)q[0][0];
 #pragma unroll
   for (int i = 1; i < NP; ++i) rmin = jmin(rmin, (double)q[i][0]);
@@ -253,7 +273,7 @@ __device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], dou
   unsigned need = 0;
 #pragma unroll
   for (int i = 0; i < NP; ++i)
-    if (pressure_near(q[i][0], q[i][1], q[i][2], q[i][3], gm1, eps) < eps) need |= 1u << i;
+    if (pressure_near(q[i][0], q[i][1], q[i][2], q[i][3], gm1, pt) < pt) need |= 1u << i;
   if (!need) return changed;
   double theta = 1.0;
 #pragma unroll 1
@@ -274,7 +294,7 @@ __device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], dou
     for (int it = 0; it < BISECTION_STEPS; ++it) {
       const double mid = xmul(0.5, xadd(lo, hi));
       const bool ok = pressure_x(xadd(a[0], xmul(mid, d0)), xadd(a[1], xmul(mid, d1)), xadd(a[2], xmul(mid, d2)),
-                                 xadd(a[3], xmul(mid, d3)), gm1) >= eps;
+                                 xadd(a[3], xmul(mid, d3)), gm1) >= pt;
       lo = ok ? mid : lo;
       hi = ok ? hi : mid;
     }
@@ -439,6 +459,8 @@ __global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
     for (int c = 0; c < 4; ++c) a[c] = P.avg[c * ld + e];
     const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
     const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+    const double pt = pressure_target<R>(eps, pa, a[3], gm1);
+    const double det_tol = sizeof(R) == 8 ? DETECTION_TOLERANCE : DETECTION_TOLERANCE_FP32;
     const int finfo = m.face_info[e];
     bool troubled = false;
     R scaled[3][4];
@@ -488,12 +510,12 @@ __global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
           const int c = cc == 0 ? 0 : 3;
           const R tr = xsub(q[(c * NP + tab::MID_NODES[f]) * ld + e], (R)a[c]);
           const R ex = abs_(xsub(minmod2(tr, scaled[f][c]), tr));
-          troubled |= (double)ex > xmul(DETECTION_TOLERANCE, fabs(a[c]));
+          troubled |= (double)ex > xmul(det_tol, fabs(a[c]));
         }
       }
     }
     const double rmin0 = P.aux[e], pmin0 = P.aux[ld + e];
-    const bool need_pos = (rmin0 < eps) || (pmin0 < eps);
+    const bool need_pos = (rmin0 < eps) || (pmin0 < pt);
     if (!troubled && !need_pos) {
       red.kr = dkey(rmin0);
       red.kp = dkey(pmin0);

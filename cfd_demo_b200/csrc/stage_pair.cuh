@@ -31,6 +31,7 @@ template <typename R>
 __device__ __noinline__ void positivity_smem(R* s, const double* a, double gm1) {
   const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
   const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+  const double pt = pressure_target<R>(eps, pa, a[3], gm1);
   double rmin = (double)s[0];
 #pragma unroll 1
   for (int i = 1; i < NP; ++i) rmin = jmin(rmin, (double)s[i]);
@@ -43,14 +44,14 @@ __device__ __noinline__ void positivity_smem(R* s, const double* a, double gm1) 
 #pragma unroll 1
   for (int i = 0; i < NP; ++i) {
     const double q0 = s[i], q1 = s[NP + i], q2 = s[2 * NP + i], q3 = s[3 * NP + i];
-    if (!(pressure_near(q0, q1, q2, q3, gm1, eps) < eps)) continue;
+    if (!(pressure_near(q0, q1, q2, q3, gm1, pt) < pt)) continue;
     const double d0 = xsub(q0, a[0]), d1 = xsub(q1, a[1]), d2 = xsub(q2, a[2]), d3 = xsub(q3, a[3]);
     double lo = 0.0, hi = 1.0;
 #pragma unroll 1
     for (int it = 0; it < BISECTION_STEPS; ++it) {
       const double mid = xmul(0.5, xadd(lo, hi));
       const bool ok = pressure_x(xadd(a[0], xmul(mid, d0)), xadd(a[1], xmul(mid, d1)), xadd(a[2], xmul(mid, d2)),
-                                 xadd(a[3], xmul(mid, d3)), gm1) >= eps;
+                                 xadd(a[3], xmul(mid, d3)), gm1) >= pt;
       lo = ok ? mid : lo;
       hi = ok ? hi : mid;
     }
