@@ -12,7 +12,11 @@ run-loop control. DOF = K * Np solution nodes (4 conserved scalars each).
 Headline `value`: DOF-steps/s of the FP32-mixed form with the state resident
 in HBM; `fp64` holds the plain FP64 form on the same workload; `l1_rho_vs_fp64`
 is the domain-averaged L1 density difference after the timed steps; `e2e`
-runs EulerSolver.run() from a pinned host state to a host result.
+runs EulerSolver.run() from a pinned host state to a host result; `adjoint`
+times the discrete adjoint of 200 RK3 steps of the Sod sensitivity study
+(400x40 quads x 2, rusanov/minmod, FP64, checkpoints every 20 steps) against
+its forward pass and against the production run loop over the same steps
+(also alone: --workload adjoint).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -446,6 +450,59 @@ def run_batch(args) -> dict:
     }
 
 
+def run_adjoint(args) -> dict:
+    """The differentiation form: the sensitivity study on the Sod tube 400x40
+    (K = 32,000, rusanov/minmod, FP64), 200 CFL steps, checkpoints every 20
+    steps. Times, with CUDA events, the forward pass of the fixed-schedule run
+    (keeping checkpoints), the backward pass (segment recompute with the tape
+    + adjoint steps), and the production run loop (EulerSolver.advance,
+    graph-replayed) over the same 200 steps."""
+    import torch
+
+    from cfd_demo_b200.adjoint import AdjointRun, SodSensitivity, cfl_schedule
+
+    torch.cuda.set_device(0)
+    steps, every = args.adjoint_steps, 20
+    case = SodSensitivity(400, 40, flux="rusanov", limiter="minmod", seed=0)
+    dev = case.solver.operators.device
+    q0 = case.initial_state(torch.tensor(case.rho_left, dtype=torch.float64, device=dev))
+    dts = cfl_schedule(case.solver, q0.cpu().numpy(), steps=steps)
+    runner = AdjointRun(case.solver, dts, checkpoint_every=every)
+    x0 = runner.pack(q0)
+    g = runner.pack(torch.stack([case.weight] + [torch.zeros_like(case.weight)] * 3, dim=-1))
+
+    def timed(fn, repeats=3):
+        fn()  # warm-up
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(repeats):
+            out = fn()
+        stop.record()
+        stop.synchronize()
+        return start.elapsed_time(stop) / repeats, out
+
+    fwd_ms, (xT, checkpoints) = timed(lambda: runner.forward(x0))
+    bwd_ms, _ = timed(lambda: runner.backward(g, checkpoints))
+    solver = case.solver
+    solver.begin_run(q0.cpu().numpy(), math.inf)
+
+    def production():
+        solver.begin_run(q0.cpu().numpy(), math.inf)
+        return solver.advance(steps)
+
+    run_ms, _ = timed(production, repeats=2)
+    return {
+        "workload": f"Sod 400x40 quads x 2 (K={solver.mesh.num_elements}), rusanov/minmod, FP64, {steps} CFL steps, "
+                    f"checkpoints every {every}",
+        "forward_ms": fwd_ms, "backward_ms": bwd_ms, "run_loop_ms": run_ms,
+        "adjoint_over_forward": bwd_ms / fwd_ms,
+        "adjoint_over_run_loop": bwd_ms / run_ms,
+        "note": "backward = segment recompute with the tape + adjoint steps; run_loop = EulerSolver.advance "
+                "(graph-replayed device run loop, includes begin_run) over the same steps",
+    }
+
+
 def run_reference(args) -> dict:
     """The reference arm: the CPU oracle (NumPy restatement of the reference's
     own algorithm; JAX is not installed) on the host cores."""
@@ -475,7 +532,9 @@ def main() -> None:
     ap.add_argument("--cpu-baseline-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="stage-kernel variant (default: autotuned)")
-    ap.add_argument("--workload", choices=["microbenchmark", "batch"], default="microbenchmark")
+    ap.add_argument("--workload", choices=["microbenchmark", "batch", "adjoint"], default="microbenchmark")
+    ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing of the default line")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-final-time", type=float, default=0.15)
     ap.add_argument("--batch-sequential", type=int, default=256)
@@ -490,6 +549,10 @@ def main() -> None:
     if args.workload == "batch":
         if rank == 0:
             print(json.dumps(run_batch(args)), flush=True)
+        return
+    if args.workload == "adjoint":
+        if rank == 0:
+            print(json.dumps(run_adjoint(args)), flush=True)
         return
 
     if args.impl == "reference":
@@ -518,6 +581,8 @@ def main() -> None:
         torch.distributed.destroy_process_group()
     if rank == 0:
         line["cpu_baseline"] = base
+        if world == 1 and not args.no_adjoint:
+            line["adjoint"] = run_adjoint(args)
         print(json.dumps(line), flush=True)
 
 

@@ -18,6 +18,7 @@ CFD_FP32_MIXED = 1
 FACE_INTERIOR, FACE_SLIP_WALL, FACE_FIXED_STATE = 0, 1, 2
 RUN_ACTIVE, RUN_DONE, RUN_BAD_DT, RUN_REJECTED = 0, 1, -1, -2
 NOALLOC_MAX_ELEMENTS = 16384  # CFD_NOALLOC_MAX_ELEMENTS of include/cfd_b200.h
+ADJ_HOLD_THETA = 1  # CFD_ADJ_HOLD_THETA
 
 _p = C.c_void_p
 _i32 = C.c_int32
@@ -79,6 +80,10 @@ _PROTOS = {
     "cfd_run_control": (C.c_int, [_SP, _p]),
     "cfd_run_init": (C.c_int, [_SP, _p, _p, _p]),
     "cfd_rk3_step_noalloc": (C.c_int, [C.POINTER(CfdMesh), _i32, _i32, _i32, _f64, _f64, _p, _p, _f64, _p, _p]),
+    "cfd_tape_bytes": (C.c_int64, [_i32, _i32]),
+    "cfd_adjoint_work_bytes": (C.c_int64, [_i32, _i32]),
+    "cfd_rk3_step_fixed": (C.c_int, [_SP, _p, _p, _p, _p, _p, _p]),
+    "cfd_rk3_step_adjoint": (C.c_int, [_SP, _p, _p, _p, _p, _p, _p, _i32, _p, _p]),
     "cfd_interface_flux": (C.c_int, [_i32, _i32, _p, _p, _p, _p, _f64, _p, _p]),
     "cfd_limiter_phi": (C.c_int, [_i32, _i32, _p, _p, _p]),
 }

@@ -1,0 +1,724 @@
+// adjoint.cuh — hand-written discrete adjoint (vector-Jacobian products) of
+// one fixed-size SSP-RK3 step: stage combine, limiters and the DG right-hand
+// side. Included by kernels.cu inside namespace cfd.
+//
+// For a stage  q' = Lambda(qt),  qt = a q_n + b (q_s + dt L(q_s))  and the
+// adjoint g of q', the backward pass computes
+//   qt_bar = Lambda'(qt)^T g                (limiter branches replayed from qt)
+//   q_n_bar += a qt_bar,   q_s_bar = b qt_bar + b dt L'(q_s)^T qt_bar.
+// dt is a constant of the step: CFD-demo's run loop converts it to a host
+// float (solver.py:181), so a gradient taken through it carries no dt term.
+//   L'(q)^T v, volume (dg.py:148-151, Ft = rx F + ry G, Gt = sx F + sy G):
+//     Ft_bar = -Dr^T v, Gt_bar = -Ds^T v, F_bar = rx Ft_bar + sx Gt_bar,
+//     G_bar = ry Ft_bar + sy Gt_bar, q_bar_j = (dF/dq)^T F_bar + (dG/dq)^T G_bar.
+//   surface (dg.py:153-164): w = Fscale LIFT^T v at the 15 face nodes, then
+//     q_bar += (d(F.n)/dq)^T w_own + (dFhat/dq-)^T (w_nbr - w_own):
+//   the neighbour evaluates Fhat(q_nbr, q_own, -n) = -Fhat(q_own, q_nbr, n), so
+//   its share is gathered from its w at the matching node instead of being
+//   scattered (no atomics). Slip walls chain through the mirror state; fixed
+//   exterior states feed the adjoint of the boundary state.
+//   Lambda'^T replays the forward decisions from the taped pre-limiting state,
+//   cell averages and nodal minima, so every branch is the one the forward
+//   step took: troubled flag, phi piece, min(1, phi), the +/- rescaling case
+//   (limiting.py:136-163); the density scaling theta with its min routed to
+//   the argmin node (limiting.py:170-181). The pressure-scaling theta is found
+//   by bisection (limiting.py:183-200), piecewise constant in q: jax.grad
+//   gives it a zero derivative (hold_theta), while the root it approximates
+//   to 2^-60 moves with q; by default its implicit derivative is used, which
+//   is what a finite difference of the forward step sees.
+// Rusanov Jacobians are analytic; Roe and HLLC use forward-mode dual numbers
+// through the same device flux code as the forward kernels.
+#pragma once
+
+// ---- forward-mode dual numbers -----------------------------------------------
+template <typename T>
+struct Dual {
+  T v, d;
+  __device__ __forceinline__ Dual() {}
+  __device__ __forceinline__ Dual(T x) : v(x), d(T(0)) {}
+  __device__ __forceinline__ Dual(T x, T dx) : v(x), d(dx) {}
+};
+template <typename T> __device__ __forceinline__ Dual<T> operator+(Dual<T> a, Dual<T> b) { return Dual<T>(a.v + b.v, a.d + b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a, Dual<T> b) { return Dual<T>(a.v - b.v, a.d - b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a) { return Dual<T>(-a.v, -a.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator*(Dual<T> a, Dual<T> b) { return Dual<T>(a.v * b.v, a.d * b.v + a.v * b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator/(Dual<T> a, Dual<T> b) {
+  const T q = a.v / b.v;
+  return Dual<T>(q, (a.d - q * b.d) / b.v);
+}
+template <typename T> __device__ __forceinline__ bool operator<(Dual<T> a, Dual<T> b) { return a.v < b.v; }
+template <typename T> __device__ __forceinline__ bool operator>(Dual<T> a, Dual<T> b) { return a.v > b.v; }
+template <typename T> __device__ __forceinline__ bool operator<=(Dual<T> a, Dual<T> b) { return a.v <= b.v; }
+template <typename T> __device__ __forceinline__ bool operator>=(Dual<T> a, Dual<T> b) { return a.v >= b.v; }
+template <typename T> __device__ __forceinline__ bool operator==(Dual<T> a, Dual<T> b) { return a.v == b.v; }
+template <typename T> __device__ __forceinline__ bool operator!=(Dual<T> a, Dual<T> b) { return a.v != b.v; }
+template <typename T> __device__ __forceinline__ Dual<T> rcp(Dual<T> x) {
+  const T r = rcp(x.v);
+  return Dual<T>(r, -x.d * r * r);
+}
+template <typename T> __device__ __forceinline__ Dual<T> sqrt_(Dual<T> x) {
+  const T s = sqrt_(x.v);
+  return Dual<T>(s, x.d * T(0.5) / s);
+}
+// |x| with derivative sign(x) dx, sign(0) = 0 (jax.numpy.abs; a central
+// difference across the kink sees 0 as well)
+template <typename T> __device__ __forceinline__ Dual<T> abs_(Dual<T> x) {
+  return Dual<T>(x.v < T(0) ? -x.v : x.v, x.v < T(0) ? -x.d : (x.v > T(0) ? x.d : T(0)));
+}
+template <typename T> __device__ __forceinline__ Dual<T> nonzero(Dual<T> x) { return Dual<T>(nonzero(x.v), x.d); }
+template <typename T> __device__ __forceinline__ Dual<T> div_(Dual<T> a, Dual<T> b) { return a / b; }
+
+// (dFhat/dq_side)^T w of the interface flux by four forward-mode evaluations
+// seeded on q- (side 0) or q+ (side 1).
+template <typename R, int FLUX>
+__device__ __forceinline__ void flux_vjp_dual(const R qm[4], const R qp[4], R nx, R ny, R gamma, const R w[4],
+                                              int side, R out[4]) {
+#pragma unroll 1
+  for (int k = 0; k < 4; ++k) {
+    Dual<R> a[4], b[4], fh[4], fm[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      a[c] = Dual<R>(qm[c], (side == 0 && c == k) ? R(1) : R(0));
+      b[c] = Dual<R>(qp[c], (side == 1 && c == k) ? R(1) : R(0));
+    }
+    interface_flux<Dual<R>, FLUX>(a, b, Dual<R>(nx), Dual<R>(ny), Dual<R>(gamma), fh, fm);
+    R s = R(0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) s += fh[c].d * w[c];
+    out[k] = s;
+  }
+}
+
+// (d(F(q).n)/dq)^T w for the Euler normal flux (euler.py:49-61), analytic.
+template <typename R>
+__device__ __forceinline__ void normal_flux_vjp(const R q[4], R nx, R ny, R gm1, const R w[4], R out[4]) {
+  const R ir = R(1) / q[0];
+  const R u = q[1] * ir, v = q[2] * ir;
+  const R un = u * nx + v * ny;
+  const R p = gm1 * (q[3] - R(0.5) * (q[1] * u + q[2] * v));
+  const R wun = w[1] * q[1] + w[2] * q[2] + w[3] * (q[3] + p);  // weight of d(un)
+  const R wp = w[1] * nx + w[2] * ny + w[3] * un;               // weight of d(p)
+  // d(un) = (-un, nx, ny, 0) / rho ;  d(p) = gm1 (|u|^2 / 2, -u, -v, 1)
+  out[0] = -wun * un * ir + wp * gm1 * R(0.5) * (u * u + v * v);
+  out[1] = w[0] * nx + wun * nx * ir - wp * gm1 * u + un * w[1];
+  out[2] = w[0] * ny + wun * ny * ir - wp * gm1 * v + un * w[2];
+  out[3] = wp * gm1 + un * w[3];
+}
+
+// s = |u.n| + c and its gradient with respect to q (Rusanov's wave speed)
+template <typename R>
+__device__ __forceinline__ void speed_grad(const R q[4], R nx, R ny, R gamma, R& s, R g[4]) {
+  const R gm1 = gamma - R(1);
+  const R ir = R(1) / q[0];
+  const R u = q[1] * ir, v = q[2] * ir;
+  const R un = u * nx + v * ny;
+  const R p = gm1 * (q[3] - R(0.5) * (q[1] * u + q[2] * v));
+  const R c = sqrt_(gamma * p * ir);
+  s = abs_(un) + c;
+  const R sg = un < R(0) ? R(-1) : (un > R(0) ? R(1) : R(0));  // d|un|, sign(0) = 0
+  const R kc = gamma * ir / (R(2) * c);  // dc = kc (dp - (p / rho) d rho)
+  g[0] = sg * (-un * ir) + kc * (gm1 * R(0.5) * (u * u + v * v) - p * ir);
+  g[1] = sg * nx * ir + kc * (-gm1 * u);
+  g[2] = sg * ny * ir + kc * (-gm1 * v);
+  g[3] = kc * gm1;
+}
+
+// Rusanov (fluxes.py:28-37): (dFhat/dq-)^T w (side 0) or (dFhat/dq+)^T w (side 1).
+template <typename R>
+__device__ __forceinline__ void rusanov_vjp(const R qm[4], const R qp[4], R nx, R ny, R gamma, const R w[4], int side,
+                                            R out[4]) {
+  R sm, sp, gm[4], gp[4];
+  speed_grad(qm, nx, ny, gamma, sm, gm);
+  speed_grad(qp, nx, ny, gamma, sp, gp);
+  const bool minus_max = sm > sp;  // alpha = max(sm, sp) as the forward flux picks it
+  const R alpha = minus_max ? sm : sp;
+  R jf[4];
+  normal_flux_vjp(side == 0 ? qm : qp, nx, ny, gamma - R(1), w, jf);
+  R wdq = R(0);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) wdq += w[c] * (qp[c] - qm[c]);
+  const bool alpha_here = side == 0 ? minus_max : !minus_max;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const R ga = alpha_here ? (side == 0 ? gm[c] : gp[c]) : R(0);
+    out[c] = R(0.5) * jf[c] + (side == 0 ? R(0.5) : R(-0.5)) * alpha * w[c] - R(0.5) * wdq * ga;
+  }
+}
+
+template <typename R, int FLUX>
+__device__ __forceinline__ void iflux_vjp(const R qm[4], const R qp[4], R nx, R ny, R gamma, const R w[4], int side,
+                                          R out[4]) {
+  if (FLUX == FLUX_RUSANOV) rusanov_vjp(qm, qp, nx, ny, gamma, w, side, out);
+  else flux_vjp_dual<R, FLUX>(qm, qp, nx, ny, gamma, w, side, out);
+}
+
+struct AdjParams {
+  CfdMesh m;
+  double gamma;
+  const double* dt;    // per-instance step size
+  const void* qt;      // pre-limiting stage state (tape)
+  const double* avg;   // its cell averages [4][ld] (tape)
+  const double* aux;   // its nodal density / pressure minima [2][ld] (tape)
+  const void* qs;      // stage input state
+  const void* g;       // adjoint of the limited stage state
+  void* qtb;           // adjoint of qt (out)
+  void* w;             // face-node adjoints [60][ld]
+  void* nab;           // adjoints of the neighbour averages [12][ld]
+  void* src_bar;       // adjoint of q_s (written or accumulated)
+  void* base_bar;      // adjoint of q_n (accumulated; null when a = 0)
+  double* bc_bar;      // [rows][4] adjoint of the fixed exterior states (accumulated; may be null)
+  double a, b;         // stage coefficients
+  int accumulate_src;  // 1: src_bar += ..., 0: src_bar = ...
+  int limited;         // troubled-cell limiter active
+  int hold_theta;      // 1: pressure-scaling theta constant (jax.grad semantics)
+};
+
+__device__ __forceinline__ int element_instance(const CfdMesh& m, int e) { return m.instance ? m.instance[e] : 0; }
+
+// ---- limiter adjoint ------------------------------------------------------------
+// phi'(r) on the piece the forward value lies on (limiters.py:16-39)
+template <typename R, int PHI>
+__device__ __forceinline__ R phi_grad(R r) {
+  if (PHI == LIM_MINMOD) return (r > R(0) && r < R(1)) ? R(1) : R(0);
+  if (PHI == LIM_MC) {
+    if (!(r > R(0))) return R(0);
+    const R a = R(2) * r, b = R(0.5) * (R(1) + r);
+    const R m = a < b ? a : b;
+    if (!(m < R(2))) return R(0);
+    return a < b ? R(2) : R(0.5);
+  }
+  if (PHI == LIM_VAN_LEER) return r > R(0) ? R(2) / ((R(1) + r) * (R(1) + r)) : R(0);
+  if (PHI == LIM_SUPERBEE) {
+    if (!(r > R(0))) return R(0);
+    const R a = (R(2) * r < R(1)) ? R(2) * r : R(1);
+    const R b = (r < R(2)) ? r : R(2);
+    if (a >= b) return R(2) * r < R(1) ? R(2) : R(0);
+    return r < R(2) ? R(1) : R(0);
+  }
+  return R(0);
+}
+
+// qt_bar = Lambda'(qt)^T g for one element, plus the adjoints of the three
+// neighbour / ghost averages it read (gathered by adj_limit_gather_kernel).
+template <typename R, int PHI>
+__global__ void __launch_bounds__(128) adj_limit_kernel(const AdjParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.num_elements || element_instance(m, e) < 0) return;
+  const R* __restrict__ qt = (const R*)P.qt;
+  const R* __restrict__ g = (const R*)P.g;
+  R* __restrict__ qtb = (R*)P.qtb;
+  R* __restrict__ nab = (R*)P.nab;
+  const double gm1 = P.gamma - 1.0;
+  double a[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) a[c] = P.avg[c * ld + e];
+  const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
+  const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+  const double pt = pressure_target<R>(eps, pa, a[3], gm1);
+  const int finfo = m.face_info[e];
+
+  // --- replay the detection exactly as limit_kernel does (limiting.py:128-151)
+  bool troubled = false;
+  R scaled[3][4];
+  if (PHI != LIM_UNLIMITED) {
+    const double det_tol = sizeof(R) == 8 ? DETECTION_TOLERANCE : DETECTION_TOLERANCE_FP32;
+    R dif[3][4];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const int kind = (finfo >> (8 * f)) & 3;
+      double na[4];
+      if (kind == CFD_FACE_INTERIOR) {
+        const int nb = m.neighbor[f * ld + e];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) na[c] = P.avg[c * ld + nb];
+      } else if (kind == CFD_FACE_SLIP_WALL) {
+        const double nx = m.face_geo[(3 * f) * ld + e], ny = m.face_geo[(3 * f + 1) * ld + e];
+        const double mn = xadd(xmul(a[1], nx), xmul(a[2], ny));
+        na[0] = a[0];
+        na[1] = xsub(a[1], xmul(xmul(2.0, mn), nx));
+        na[2] = xsub(a[2], xmul(xmul(2.0, mn), ny));
+        na[3] = a[3];
+      } else {
+        const int row = m.neighbor[f * ld + e];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) na[c] = m.bc_states[row * 4 + c];
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dif[f][c] = (R)xsub(na[c], a[c]);
+    }
+    const R* __restrict__ cs = GeoPtr<R>::cs(m);
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const int pf = (finfo >> (8 * f + 4)) & 3;
+      const R al = cs[f * ld + e], be = cs[(3 + f) * ld + e];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const R pd = pf == 0 ? dif[0][c] : (pf == 1 ? dif[1][c] : dif[2][c]);
+        scaled[f][c] = xmul((R)NEIGHBOR_FACTOR, xadd(xmul(al, dif[f][c]), xmul(be, pd)));
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+      for (int cc = 0; cc < 2; ++cc) {
+        const int c = cc == 0 ? 0 : 3;
+        const R tr = xsub(qt[(c * NP + tab::MID_NODES[f]) * ld + e], (R)a[c]);
+        const R ex = abs_(xsub(minmod2(tr, scaled[f][c]), tr));
+        troubled |= (double)ex > xmul(det_tol, fabs(a[c]));
+      }
+  }
+  const bool need_pos = (P.aux[e] < eps) || (P.aux[ld + e] < pt);
+  if (!troubled && !need_pos) {  // the limiters left the element as it was
+#pragma unroll 1
+    for (int k = 0; k < 4 * NP; ++k) qtb[k * ld + e] = g[k * ld + e];
+    if (PHI != LIM_UNLIMITED) {
+#pragma unroll 1
+      for (int k = 0; k < 12; ++k) nab[k * ld + e] = R(0);
+    }
+    return;
+  }
+
+  R s[NP][4];
+#pragma unroll
+  for (int i = 0; i < NP; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) s[i][c] = qt[(c * NP + i) * ld + e];
+  // --- forward troubled-cell reconstruction, keeping what the reverse needs
+  R proj[3][4], mfac[3][4], del[3][4], thp[4], thn[4], pos[4], neg[4];
+  if (troubled) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const R ac = (R)a[c];
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        R pr = xmul((R)tab::P1MID[f][0], s[0][c]);
+#pragma unroll
+        for (int i = 1; i < NP; ++i) pr = xadd(pr, xmul((R)tab::P1MID[f][i], s[i][c]));
+        pr = xsub(pr, ac);
+        proj[f][c] = pr;
+        R d = R(0), mf = R(0);
+        if (pr != R(0)) {
+          mf = jmin(R(1), phi<R, PHI>(xdiv(scaled[f][c], pr)));
+          d = xmul(pr, mf);
+        }
+        mfac[f][c] = mf;
+        del[f][c] = d;
+        pos[c] = f == 0 ? jmax(d, R(0)) : xadd(pos[c], jmax(d, R(0)));
+        neg[c] = f == 0 ? jmax(-d, R(0)) : xadd(neg[c], jmax(-d, R(0)));
+      }
+      thp[c] = pos[c] > R(0) ? jmin(R(1), xdiv(neg[c], pos[c])) : R(0);
+      thn[c] = neg[c] > R(0) ? jmin(R(1), xdiv(pos[c], neg[c])) : R(0);
+      R dl[3];
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+        dl[f] = xsub(xmul(thp[c], jmax(del[f][c], R(0))), xmul(thn[c], jmax(-del[f][c], R(0))));
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        R v = xmul((R)tab::LINBASIS[i][0], dl[0]);
+        v = xadd(v, xmul((R)tab::LINBASIS[i][1], dl[1]));
+        v = xadd(v, xmul((R)tab::LINBASIS[i][2], dl[2]));
+        s[i][c] = xadd(ac, v);
+      }
+    }
+  }
+  // --- forward positivity decisions (the order of positivity() in kernels.cu)
+  int imin = 0;
+  double rmin = (double)s[0][0];
+#pragma unroll
+  for (int i = 1; i < NP; ++i) {
+    const double r = (double)s[i][0];
+    imin = r < rmin ? i : imin;
+    rmin = jmin(rmin, r);
+  }
+  double th1 = 1.0;
+  bool dens = false, dclip = true;
+  if (rmin < eps) {
+    dens = true;
+    const double raw = xdiv(xsub(a[0], eps), xsub(a[0], rmin));
+    th1 = jmin(jmax(raw, 0.0), 1.0);
+    dclip = !(raw > 0.0 && raw < 1.0);
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s[i][c] = (R)xadd(a[c], xmul(th1, xsub((double)s[i][c], a[c])));
+  }
+  double th2 = 1.0;
+  int i2 = -1;  // the node whose bisection set th2
+#pragma unroll 1
+  for (int i = 0; i < NP; ++i) {
+    double qi[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double v = 0.0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) v = (j == i) ? (double)s[j][c] : v;
+      qi[c] = v;
+    }
+    if (!(pressure_near(qi[0], qi[1], qi[2], qi[3], gm1, pt) < pt)) continue;
+    const double d0 = xsub(qi[0], a[0]), d1 = xsub(qi[1], a[1]), d2 = xsub(qi[2], a[2]), d3 = xsub(qi[3], a[3]);
+    double lo = 0.0, hi = 1.0;
+#pragma unroll 1
+    for (int it = 0; it < BISECTION_STEPS; ++it) {
+      const double mid = xmul(0.5, xadd(lo, hi));
+      const bool ok = pressure_x(xadd(a[0], xmul(mid, d0)), xadd(a[1], xmul(mid, d1)), xadd(a[2], xmul(mid, d2)),
+                                 xadd(a[3], xmul(mid, d3)), gm1) >= pt;
+      lo = ok ? mid : lo;
+      hi = ok ? hi : mid;
+    }
+    if (lo < th2) i2 = i;
+    th2 = jmin(th2, lo);
+  }
+  if (!(th2 < 1.0)) th2 = 1.0;
+
+  // --- reverse pass; y is the running adjoint of the nodal state, abar that
+  // of the cell averages (which are AVG_W-weighted sums of qt)
+  R y[NP][4];
+#pragma unroll
+  for (int i = 0; i < NP; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) y[i][c] = g[(c * NP + i) * ld + e];
+  R abar[4] = {R(0), R(0), R(0), R(0)};
+  // pressure scaling out = a + th2 (in - a). th2 is the bisection root of
+  // p(a + th (in_i2 - a)) = pt at the critical node i2: held constant (the
+  // derivative of the bisection itself), or differentiated implicitly,
+  //   d th2 = -grad p(z) . ((1 - th2) da + th2 d in_i2) / (grad p(z) . (in_i2 - a)),
+  // z = a + th2 (in_i2 - a), which follows the root the bisection resolves to
+  // 2^-60 (pt held constant, like eps).
+  if (th2 < 1.0) {
+    R thbar = R(0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      R sum = R(0);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        thbar += (R)((double)s[i][c] - a[c]) * y[i][c];
+        sum += y[i][c];
+        y[i][c] *= (R)th2;
+      }
+      abar[c] += (R)(1.0 - th2) * sum;
+    }
+    if (!P.hold_theta && i2 >= 0) {
+      double d[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) v = (j == i2) ? (double)s[j][c] : v;
+        d[c] = v - a[c];
+      }
+      const double z0 = a[0] + th2 * d[0], u = (a[1] + th2 * d[1]) / z0, v = (a[2] + th2 * d[2]) / z0;
+      const double gp[4] = {gm1 * 0.5 * (u * u + v * v), -gm1 * u, -gm1 * v, gm1};  // grad p(z)
+      const double den = gp[0] * d[0] + gp[1] * d[1] + gp[2] * d[2] + gp[3] * d[3];
+      if (den != 0.0) {
+        const double k = -(double)thbar / den;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          abar[c] += (R)(k * (1.0 - th2) * gp[c]);
+#pragma unroll
+          for (int i = 0; i < NP; ++i)
+            if (i == i2) y[i][c] += (R)(k * th2 * gp[c]);
+        }
+      }
+    }
+  }
+  // density scaling out = a + th1 (in - a), th1 = (a_rho - eps) / (a_rho - min_i rho_i)
+  if (dens) {
+    R thbar = R(0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      R sum = R(0);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const R din = th1 > 0.0 ? (R)(((double)s[i][c] - a[c]) / th1) : R(0);  // in - a
+        thbar += din * y[i][c];
+        sum += y[i][c];
+        y[i][c] *= (R)th1;
+      }
+      abar[c] += (R)(1.0 - th1) * sum;
+    }
+    if (!dclip) {
+      const double span = a[0] - rmin;
+      const R dth_da = (R)((eps - rmin) / (span * span));
+      const R dth_dmin = (R)((a[0] - eps) / (span * span));
+      abar[0] += thbar * dth_da;
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+        if (i == imin) y[i][0] += thbar * dth_dmin;
+    }
+  }
+  // troubled-cell reconstruction
+  R nabar[3][4];
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) nabar[f][c] = R(0);
+  if (troubled) {
+    const R* __restrict__ cs = GeoPtr<R>::cs(m);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      R ab = R(0), dpb[3] = {R(0), R(0), R(0)};
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        ab += y[i][c];
+#pragma unroll
+        for (int f = 0; f < 3; ++f) dpb[f] += (R)tab::LINBASIS[i][f] * y[i][c];
+        y[i][c] = R(0);  // a rebuilt element depends on its nodes only through the P1 projections
+      }
+      R thpb = R(0), thnb = R(0), pb[3], nb_[3];
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        pb[f] = thp[c] * dpb[f];
+        nb_[f] = -thn[c] * dpb[f];
+        thpb += jmax(del[f][c], R(0)) * dpb[f];
+        thnb -= jmax(-del[f][c], R(0)) * dpb[f];
+      }
+      R posb = R(0), negb = R(0);
+      if (pos[c] > R(0) && neg[c] < pos[c]) {  // thp = neg / pos below the cap
+        negb += thpb / pos[c];
+        posb -= thpb * neg[c] / (pos[c] * pos[c]);
+      }
+      if (neg[c] > R(0) && pos[c] < neg[c]) {  // thn = pos / neg below the cap
+        posb += thnb / neg[c];
+        negb -= thnb * pos[c] / (neg[c] * neg[c]);
+      }
+      R difb[3] = {R(0), R(0), R(0)};
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        const R d = del[f][c];
+        const R delb = d > R(0) ? pb[f] + posb : (d < R(0) ? -(nb_[f] + negb) : R(0));
+        R projb = R(0), scb = R(0);
+        const R pr = proj[f][c];
+        if (pr != R(0)) {
+          projb = mfac[f][c] * delb;
+          const R r = scaled[f][c] / pr;
+          const R rb = phi<R, PHI>(r) < R(1) ? phi_grad<R, PHI>(r) * pr * delb : R(0);
+          scb = rb / pr;
+          projb -= rb * scaled[f][c] / (pr * pr);
+        }
+        // proj_f = P1MID_f . q - a ; scaled_f = 1.5 (alpha_f dif_f + beta_f dif_pf), dif = na - a
+        ab -= projb;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) y[i][c] += (R)tab::P1MID[f][i] * projb;
+        const int pf = (finfo >> (8 * f + 4)) & 3;
+        const R al = cs[f * ld + e], be = cs[(3 + f) * ld + e];
+        difb[f] += (R)NEIGHBOR_FACTOR * al * scb;
+        const R t = (R)NEIGHBOR_FACTOR * be * scb;
+        if (pf == 0) difb[0] += t;
+        else if (pf == 1) difb[1] += t;
+        else difb[2] += t;
+      }
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        nabar[f][c] = difb[f];
+        ab -= difb[f];
+      }
+      abar[c] += ab;
+    }
+    // ghost averages: a slip wall mirrors this element's average; a fixed
+    // exterior state is a boundary parameter
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const int kind = (finfo >> (8 * f)) & 3;
+      if (kind == CFD_FACE_SLIP_WALL) {
+        const R nx = (R)m.face_geo[(3 * f) * ld + e], ny = (R)m.face_geo[(3 * f + 1) * ld + e];
+        const R dm = nabar[f][1] * nx + nabar[f][2] * ny;
+        abar[0] += nabar[f][0];
+        abar[1] += nabar[f][1] - R(2) * dm * nx;
+        abar[2] += nabar[f][2] - R(2) * dm * ny;
+        abar[3] += nabar[f][3];
+      } else if (kind == CFD_FACE_FIXED_STATE && P.bc_bar) {
+        const int row = m.neighbor[f * ld + e];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (nabar[f][c] != R(0)) atomicAdd(&P.bc_bar[row * 4 + c], (double)nabar[f][c]);
+      }
+      if (kind != CFD_FACE_INTERIOR) nabar[f][0] = nabar[f][1] = nabar[f][2] = nabar[f][3] = R(0);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NP; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qtb[(c * NP + i) * ld + e] = y[i][c] + (R)tab::AVG_W[i] * abar[c];
+  if (PHI != LIM_UNLIMITED) {
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) nab[(f * 4 + c) * ld + e] = nabar[f][c];
+  }
+}
+
+// adds the neighbours' adjoints of this element's average to qt_bar
+template <typename R>
+__global__ void __launch_bounds__(128) adj_limit_gather_kernel(const AdjParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.num_elements || element_instance(m, e) < 0) return;
+  const R* __restrict__ nab = (const R*)P.nab;
+  R* __restrict__ qtb = (R*)P.qtb;
+  const int finfo = m.face_info[e];
+  R ab[4] = {R(0), R(0), R(0), R(0)};
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const int info = (finfo >> (8 * f)) & 0xff;
+    if ((info & 3) != CFD_FACE_INTERIOR) continue;
+    const int nb = m.neighbor[f * ld + e];
+    const int nf = (info >> 2) & 3;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ab[c] += nab[(nf * 4 + c) * ld + nb];
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (ab[c] == R(0)) continue;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) qtb[(c * NP + i) * ld + e] += (R)tab::AVG_W[i] * ab[c];
+  }
+}
+
+// surface pass A: w = b dt Fscale LIFT^T qt_bar at the 15 face nodes
+template <typename R>
+__global__ void __launch_bounds__(128) adj_rhs_a_kernel(const AdjParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.num_elements) return;
+  const int inst = element_instance(m, e);
+  if (inst < 0) return;
+  const R* __restrict__ v = (const R*)P.qtb;
+  R* __restrict__ w = (R*)P.w;
+  const R scale = (R)(P.b * P.dt[inst]);
+  R fs[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) fs[f] = scale * (R)m.face_geo[(3 * f + 2) * ld + e];
+#pragma unroll 1
+  for (int c = 0; c < 4; ++c) {
+    R vi[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) vi[i] = v[(c * NP + i) * ld + e];
+#pragma unroll
+    for (int col = 0; col < 3 * NFP; ++col) {
+      R t = R(0);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) t = fma((R)tab::LIFT[i][col], vi[i], t);
+      w[(c * NP + col) * ld + e] = fs[col / NFP] * t;
+    }
+  }
+}
+
+// pass B: the adjoints of the stage input (volume + surface) and of the base state
+template <typename R, int FLUX>
+__global__ void __launch_bounds__(128) adj_rhs_b_kernel(const AdjParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.num_elements) return;
+  const int inst = element_instance(m, e);
+  if (inst < 0) return;
+  const R* __restrict__ qs = (const R*)P.qs;
+  const R* __restrict__ qtb = (const R*)P.qtb;
+  const R* __restrict__ w = (const R*)P.w;
+  R* __restrict__ sb = (R*)P.src_bar;
+  R* __restrict__ bb = (R*)P.base_bar;
+  const R gamma = (R)P.gamma, gm1 = gamma - R(1);
+  const R scale = (R)(P.b * P.dt[inst]);
+  const R rx = (R)m.metric[e], ry = (R)m.metric[ld + e], sx = (R)m.metric[2 * ld + e], sy = (R)m.metric[3 * ld + e];
+  if (bb) {
+#pragma unroll 1
+    for (int k = 0; k < 4 * NP; ++k) bb[k * ld + e] += (R)P.a * qtb[k * ld + e];
+  }
+  // volume
+#pragma unroll 1
+  for (int j = 0; j < NP; ++j) {
+    R fb[4], gb[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      R sf = R(0), sg = R(0);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const R vi = qtb[(c * NP + i) * ld + e];
+        sf = fma((R)ctab::DR[i][j], vi, sf);
+        sg = fma((R)ctab::DS[i][j], vi, sg);
+      }
+      const R ftb = -scale * sf, gtb = -scale * sg;
+      fb[c] = rx * ftb + sx * gtb;
+      gb[c] = ry * ftb + sy * gtb;
+    }
+    R q[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) q[c] = qs[(c * NP + j) * ld + e];
+    R jf[4], jg[4];
+    normal_flux_vjp(q, R(1), R(0), gm1, fb, jf);
+    normal_flux_vjp(q, R(0), R(1), gm1, gb, jg);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int idx = (c * NP + j) * ld + e;
+      const R val = (R)P.b * qtb[idx] + jf[c] + jg[c];
+      sb[idx] = P.accumulate_src ? sb[idx] + val : val;
+    }
+  }
+  // surface
+  const int finfo = m.face_info[e];
+#pragma unroll 1
+  for (int sl = 0; sl < 3 * NFP; ++sl) {
+    const int f = sl / NFP, k = sl - f * NFP;
+    const int info = (finfo >> (8 * f)) & 0xff;
+    const int kind = info & 3;
+    const R nx = (R)m.face_geo[(3 * f) * ld + e], ny = (R)m.face_geo[(3 * f + 1) * ld + e];
+    const int n = face_node_rt(f, k);
+    R qm[4], qp[4], wo[4], jfm[4], contrib[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      qm[c] = qs[(c * NP + n) * ld + e];
+      wo[c] = w[(c * NP + sl) * ld + e];
+    }
+    normal_flux_vjp(qm, nx, ny, gm1, wo, jfm);
+    if (kind == CFD_FACE_INTERIOR) {
+      const int nb = m.neighbor[f * ld + e];
+      const int nf = (info >> 2) & 3;
+      const int kk = ((f == 2) == (nf == 2)) ? NFP - 1 - k : k;
+      const int pn = face_node_rt(nf, kk);
+      R wd[4], jm[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        qp[c] = qs[(c * NP + pn) * ld + nb];
+        wd[c] = w[(c * NP + nf * NFP + kk) * ld + nb] - wo[c];
+      }
+      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wd, 0, jm);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) contrib[c] = jfm[c] + jm[c];
+    } else if (kind == CFD_FACE_SLIP_WALL) {
+      const R mn = qm[1] * nx + qm[2] * ny;
+      qp[0] = qm[0];
+      qp[1] = qm[1] - R(2) * mn * nx;
+      qp[2] = qm[2] - R(2) * mn * ny;
+      qp[3] = qm[3];
+      R jm[4], jp[4];
+      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 0, jm);
+      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 1, jp);
+      // q+ = M q- with M = M^T (the normal momentum reversed)
+      const R dm = jp[1] * nx + jp[2] * ny;
+      contrib[0] = jfm[0] - jm[0] - jp[0];
+      contrib[1] = jfm[1] - jm[1] - (jp[1] - R(2) * dm * nx);
+      contrib[2] = jfm[2] - jm[2] - (jp[2] - R(2) * dm * ny);
+      contrib[3] = jfm[3] - jm[3] - jp[3];
+    } else {
+      const int row = m.neighbor[f * ld + e];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
+      R jm[4];
+      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 0, jm);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) contrib[c] = jfm[c] - jm[c];
+      if (P.bc_bar) {
+        R jp[4];
+        iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 1, jp);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) atomicAdd(&P.bc_bar[row * 4 + c], -(double)jp[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) sb[(c * NP + n) * ld + e] += contrib[c];
+  }
+}

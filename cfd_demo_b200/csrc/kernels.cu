@@ -617,6 +617,8 @@ __global__ void __launch_bounds__(BS) prep_kernel(CfdMesh m, const R* __restrict
   aux[2 * ld + e] = lam;
 }
 
+#include "adjoint.cuh"
+
 // ---------------------------------------------------------- small kernels ---
 template <typename R, int BS>
 __global__ void __launch_bounds__(BS) dt_kernel(CfdMesh m, const R* __restrict__ q, CfdStageAcc* acc, double gamma,
@@ -760,6 +762,21 @@ __global__ void run_init_kernel(CfdControl* ctl, const CfdStageAcc* acc, const d
       c.dt = c.reaches_end ? remaining : dt;
     }
   }
+  ctl[i] = c;
+}
+
+// Loop state of a fixed-size step (cfd_rk3_step_fixed): every instance
+// active, its state in x0, the step size given per instance.
+__global__ void fixed_control_kernel(CfdControl* ctl, const double* dt, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  CfdControl c;
+  memset(&c, 0, sizeof(c));
+  c.final_time = INFINITY;
+  c.dt = dt[i];
+  c.min_density = INFINITY;
+  c.min_pressure = INFINITY;
+  c.status = CFD_RUN_ACTIVE;
   ctl[i] = c;
 }
 
@@ -1221,6 +1238,172 @@ int cfd_limiter_phi(int32_t limiter, int32_t n, const double* r, double* out, vo
     default: return fail(CFD_E_ARG, "cfd_limiter_phi: unknown limiter id");
   }
   return check_launch("cfd_limiter_phi");
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ fixed-size step + adjoint ---
+// Tape of one step (sizes in elements of ld): the pre-limiting stage states
+// qt1, qt2, qt3 and the limited stage states q1, q2 (60 rows each, solver
+// precision) in the order qt1 q1 qt2 q2 qt3, then the cell averages of
+// qt1..qt3 (4 rows of double each) and their nodal density / pressure minima
+// (2 rows of double each).
+namespace {
+size_t state_bytes(int ld, int precision) { return (size_t)60 * ld * (precision == CFD_FP64 ? 8 : 4); }
+size_t tape_bytes(int ld, int precision) { return 5 * state_bytes(ld, precision) + (size_t)18 * ld * 8; }
+char* tape_state(void* tape, int ld, int precision, int slot) { return (char*)tape + slot * state_bytes(ld, precision); }
+double* tape_avg(void* tape, int ld, int precision, int k) {
+  return (double*)((char*)tape + 5 * state_bytes(ld, precision)) + (size_t)(k - 1) * 4 * ld;
+}
+double* tape_aux(void* tape, int ld, int precision, int k) {
+  return (double*)((char*)tape + 5 * state_bytes(ld, precision)) + (size_t)12 * ld + (size_t)(k - 1) * 2 * ld;
+}
+// adjoint scratch: qt_bar, face-node adjoints w, neighbour-average adjoints,
+// and the adjoints of q1 and q2 (60 + 60 + 12 + 60 + 60 rows)
+size_t adjoint_work_bytes(int ld, int precision) { return (size_t)252 * ld * (precision == CFD_FP64 ? 8 : 4); }
+
+template <typename R>
+void launch_adj_limit(const AdjParams& p, int lim, unsigned g, cudaStream_t st) {
+  switch (lim) {
+    case 0: adj_limit_kernel<R, 0><<<g, 128, 0, st>>>(p); break;
+    case 1: adj_limit_kernel<R, 1><<<g, 128, 0, st>>>(p); break;
+    case 2: adj_limit_kernel<R, 2><<<g, 128, 0, st>>>(p); break;
+    case 3: adj_limit_kernel<R, 3><<<g, 128, 0, st>>>(p); break;
+    default: adj_limit_kernel<R, 4><<<g, 128, 0, st>>>(p); break;
+  }
+}
+template <typename R>
+void launch_adj_rhs(const AdjParams& p, int flux, unsigned g, cudaStream_t st) {
+  adj_rhs_a_kernel<R><<<g, 128, 0, st>>>(p);
+  switch (flux) {
+    case 0: adj_rhs_b_kernel<R, 0><<<g, 128, 0, st>>>(p); break;
+    case 1: adj_rhs_b_kernel<R, 1><<<g, 128, 0, st>>>(p); break;
+    default: adj_rhs_b_kernel<R, 2><<<g, 128, 0, st>>>(p); break;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int64_t cfd_tape_bytes(int32_t ld, int32_t precision) {
+  if (ld <= 0 || (precision != CFD_FP64 && precision != CFD_FP32_MIXED)) return -1;
+  return (int64_t)tape_bytes(ld, precision);
+}
+
+int64_t cfd_adjoint_work_bytes(int32_t ld, int32_t precision) {
+  if (ld <= 0 || (precision != CFD_FP64 && precision != CFD_FP32_MIXED)) return -1;
+  return (int64_t)adjoint_work_bytes(ld, precision);
+}
+
+int cfd_rk3_step_fixed(const CfdSolver* s, const void* q_in, void* q_out, void* stage, const double* dt, void* tape,
+                       void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q_in || !q_out || !stage || !dt || !s->acc || !s->control || !s->report || !s->averages || !s->element_aux)
+    return fail(CFD_E_ARG, "cfd_rk3_step_fixed: null pointer");
+  if (q_in == q_out || q_in == stage || q_out == stage) return fail(CFD_E_ARG, "cfd_rk3_step_fixed: state buffers must be distinct");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = s->mesh.num_instances, ld = s->mesh.ld, prec = s->precision;
+  fixed_control_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->control, dt, n);
+  reset_acc(s, st);
+  const size_t sb = state_bytes(ld, prec);
+  for (int k = 1; k <= 3; ++k) {
+    StageParams p;
+    memset(&p, 0, sizeof(p));
+    p.m = s->mesh;
+    p.ctl = s->control;
+    p.x0 = q_in;
+    p.x1 = q_out;
+    p.stage = stage;
+    p.stage_idx = k;
+    p.gamma = s->gamma;
+    p.avg = s->averages;
+    p.aux = s->element_aux;
+    p.acc = s->acc;
+    // the limited path for every limiter: positivity runs in limit_kernel on
+    // the stored stage state, so the tape sees the state before limiting
+    launch_stage(s, p, MODE_LIMITED, st);
+    void* dst = k == 2 ? stage : q_out;
+    if (tape) {
+      if (cudaMemcpyAsync(tape_state(tape, ld, prec, 2 * (k - 1)), dst, sb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(tape_avg(tape, ld, prec, k), s->averages, (size_t)4 * ld * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(tape_aux(tape, ld, prec, k), s->element_aux, (size_t)2 * ld * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return check_launch("cfd_rk3_step_fixed: tape copy");
+    }
+    LimitParams lp;
+    memset(&lp, 0, sizeof(lp));
+    lp.m = s->mesh;
+    lp.ctl = s->control;
+    lp.x0 = q_in;
+    lp.x1 = q_out;
+    lp.stage = stage;
+    lp.stage_idx = k;
+    lp.gamma = s->gamma;
+    lp.avg = s->averages;
+    lp.aux = s->element_aux;
+    lp.acc = s->acc;
+    launch_limit(s, lp, st);
+    if (tape && k < 3) {
+      if (cudaMemcpyAsync(tape_state(tape, ld, prec, 2 * k - 1), dst, sb, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return check_launch("cfd_rk3_step_fixed: tape copy");
+    }
+  }
+  report_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, s->control, s->report, n, s->cfl);
+  return check_launch("cfd_rk3_step_fixed");
+}
+
+int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape, const double* dt, const void* g_out,
+                         void* g_in, double* bc_bar, int32_t flags, void* work, void* stream) {
+  int rc = validate(s);
+  if (rc) return rc;
+  if (!q_in || !tape || !dt || !g_out || !g_in || !work) return fail(CFD_E_ARG, "cfd_rk3_step_adjoint: null pointer");
+  if (g_out == g_in) return fail(CFD_E_ARG, "cfd_rk3_step_adjoint: g_in must not alias g_out");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int ld = s->mesh.ld, prec = s->precision;
+  const size_t sb = state_bytes(ld, prec), es = prec == CFD_FP64 ? 8 : 4;
+  char* wk = (char*)work;
+  void* qtb = wk;
+  void* w = wk + sb;
+  void* nab = wk + 2 * sb;
+  void* b1 = wk + 2 * sb + (size_t)12 * ld * es;  // adjoint of q1
+  void* b2 = (char*)b1 + sb;                      // adjoint of q2
+  void* tp = const_cast<void*>(tape);
+  if (cudaMemsetAsync(g_in, 0, sb, st) != cudaSuccess) return check_launch("cfd_rk3_step_adjoint: memset");
+  const unsigned g = blocks_for(s->mesh.num_elements, 128);
+  static const double A[4] = {0.0, 0.0, 0.75, 1.0 / 3.0}, B[4] = {0.0, 1.0, 0.25, 2.0 / 3.0};
+  for (int k = 3; k >= 1; --k) {
+    AdjParams p;
+    memset(&p, 0, sizeof(p));
+    p.m = s->mesh;
+    p.gamma = s->gamma;
+    p.dt = dt;
+    p.qt = tape_state(tp, ld, prec, 2 * (k - 1));
+    p.avg = tape_avg(tp, ld, prec, k);
+    p.aux = tape_aux(tp, ld, prec, k);
+    p.qs = k == 1 ? q_in : tape_state(tp, ld, prec, 2 * k - 3);
+    p.g = k == 3 ? g_out : (k == 2 ? b2 : b1);
+    p.qtb = qtb;
+    p.w = w;
+    p.nab = nab;
+    p.src_bar = k == 3 ? b2 : (k == 2 ? b1 : g_in);
+    p.base_bar = k == 1 ? nullptr : g_in;
+    p.bc_bar = bc_bar;
+    p.a = A[k];
+    p.b = B[k];
+    p.accumulate_src = k == 1;
+    p.limited = s->limiter != CFD_LIMITER_UNLIMITED;
+    p.hold_theta = (flags & CFD_ADJ_HOLD_THETA) != 0;
+    if (prec == CFD_FP64) {
+      launch_adj_limit<double>(p, s->limiter, g, st);
+      if (p.limited) adj_limit_gather_kernel<double><<<g, 128, 0, st>>>(p);
+      launch_adj_rhs<double>(p, s->flux, g, st);
+    } else {
+      launch_adj_limit<float>(p, s->limiter, g, st);
+      if (p.limited) adj_limit_gather_kernel<float><<<g, 128, 0, st>>>(p);
+      launch_adj_rhs<float>(p, s->flux, g, st);
+    }
+  }
+  return check_launch("cfd_rk3_step_adjoint");
 }
 
 }  // extern "C"

@@ -254,6 +254,43 @@ int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, v
 int cfd_rk3_step_noalloc(const CfdMesh* mesh, int32_t flux, int32_t limiter, int32_t precision, double gamma,
                          double cfl, const void* q_in, void* q_out, double dt, CfdStepReport* report, void* stream);
 
+/*
+ * ---- discrete adjoint of the fixed-size RK3 step
+ * The reference differentiates its step with jax.grad (fluxes.py:7 and
+ * limiters.py:4 keep the code differentiable; solver.py:181 turns dt into a
+ * host float, so dt is a constant of each step). These entries are its
+ * hand-written replacement for EulerSolver._step (time_integration.py:44-84)
+ * and its vector-Jacobian product; neither has a C counterpart in the
+ * reference.
+ *
+ * cfd_rk3_step_fixed: one SSP-RK3 step of size dt[instance] (device array)
+ * from q_in to q_out without CFL control or rejection; `stage` is scratch of
+ * one state. The step report is left in s->report. When `tape` is not NULL it
+ * receives what the adjoint needs (cfd_tape_bytes(ld, precision) bytes): the
+ * stage states before and after limiting and the stage averages and minima.
+ * The limiter of every configuration runs in its own kernel here, so the
+ * result can differ in the last bits from cfd_rk3_attempt's fused positivity
+ * for `unlimited`.
+ *
+ * cfd_rk3_step_adjoint: given the adjoint g_out of q_out, writes the adjoint
+ * g_in of q_in (g_in = (dq_out/dq_in)^T g_out) for the step that produced
+ * `tape` from q_in with the same dt, and adds the adjoint of the fixed
+ * exterior states to bc_bar[rows][4] when bc_bar is not NULL (the caller
+ * zeroes it). The limiter branches are those the forward step took. The
+ * pressure-scaling theta of the positivity limiter (a bisection root) is
+ * differentiated implicitly, as a finite difference of the step sees it; with
+ * CFD_ADJ_HOLD_THETA in `flags` it is held constant instead, the derivative
+ * jax.grad takes of the bisection loop. `work` is scratch of
+ * cfd_adjoint_work_bytes(ld, precision) bytes.
+ */
+#define CFD_ADJ_HOLD_THETA 1
+int64_t cfd_tape_bytes(int32_t ld, int32_t precision);
+int64_t cfd_adjoint_work_bytes(int32_t ld, int32_t precision);
+int cfd_rk3_step_fixed(const CfdSolver* s, const void* q_in, void* q_out, void* stage, const double* dt, void* tape,
+                       void* stream);
+int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape, const double* dt, const void* g_out,
+                         void* g_in, double* bc_bar, int32_t flags, void* work, void* stream);
+
 /* ---- pointwise physics (exercise the device functions of the fused kernels) */
 int cfd_interface_flux(int32_t flux, int32_t n, const double* q_minus, const double* q_plus,
                        const double* nx, const double* ny, double gamma, double* out, void* stream);

@@ -171,7 +171,7 @@ def test_library_exports_every_declared_symbol():
 
     lib = _native.load()
     header = open(os.path.join(ROOT, "include", "cfd_b200.h")).read()
-    declared = sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(cfd_\w+)\s*\(", header, re.M)))
+    declared = sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(cfd_\w+)\s*\(", header, re.M)))
     assert declared, "no declarations found"
     for name in declared:
         assert hasattr(lib, name), name
@@ -197,6 +197,21 @@ def test_argument_errors_are_reported_without_a_gpu():
     assert b"null solver" in lib.cfd_last_error()
     assert lib.cfd_interface_flux(7, 1, 1, 1, 1, 1, 1.4, 1, None) == -1
     assert lib.cfd_limiter_phi(0, -1, None, None, None) == -1
+    assert lib.cfd_rk3_step_fixed(None, None, None, None, None, None, None) == -1
+    assert lib.cfd_rk3_step_adjoint(None, None, None, None, None, None, None, 0, None, None) == -1
+
+
+def test_adjoint_buffer_sizes():
+    from cfd_demo_b200 import _native
+
+    lib = _native.load()
+    ld = 128
+    # tape: five stage states (before / after limiting) + 3 x (4 averages + 2 minima) doubles
+    assert lib.cfd_tape_bytes(ld, _native.CFD_FP64) == 5 * 60 * ld * 8 + 18 * ld * 8
+    assert lib.cfd_tape_bytes(ld, _native.CFD_FP32_MIXED) == 5 * 60 * ld * 4 + 18 * ld * 8
+    assert lib.cfd_adjoint_work_bytes(ld, _native.CFD_FP64) == 252 * ld * 8
+    assert lib.cfd_tape_bytes(0, _native.CFD_FP64) == -1
+    assert lib.cfd_adjoint_work_bytes(ld, 9) == -1
 
 
 def test_package_has_no_oracle_dependency():
