@@ -16,7 +16,9 @@ runs EulerSolver.run() from a pinned host state to a host result; `adjoint`
 times the discrete adjoint of 200 RK3 steps of the Sod sensitivity study
 (400x40 quads x 2, rusanov/minmod, FP64, checkpoints every 20 steps) against
 its forward pass and against the production run loop over the same steps
-(also alone: --workload adjoint).
+(also alone: --workload adjoint). `--workload precision` runs the precision
+study (Sod 2000x200, hllc/van_leer, t = 0.2, FP32-mixed against FP64) and
+`--workload batch` the batched Riemann instances.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -54,6 +56,16 @@ FALLBACK_HBM_GBS = 6650.0
 # per-element geometry (4 metric + 9 face values + face_info + 3 neighbour ids,
 # + dt_geo in stage 3). Neighbour-trace gathers are counted once (in the
 # neighbour's own read).
+# DRAM bytes per element of each stage launch (dram__bytes_read.sum +
+# dram__bytes_write.sum) measured by ncu on the tiled stage kernel at 512x512
+# quads (K = 524,288; the 724x724 workload is too large for a full capture),
+# scaled to a launch of the benchmark by its element count (traffic grows in
+# proportion to K): profiles/stage_tile_fp32_512x512.md and
+# profiles/stage_tile_fp64_512x512.md. Writes still in L2 when a launch ends
+# are not counted there, so the stage result's 240 / 480 B appear partly.
+NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (482.2, 741.1, 748.2), "fp64": (1011.6, 1516.0, 1524.7)}
+
+
 def stage_bytes(real_bytes: int) -> list[int]:
     state = 60 * real_bytes
     geo = 13 * real_bytes + 4 + 12
@@ -161,11 +173,33 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
-        time.sleep(0.3)
+        # the timed region starts only once nvidia-smi is sampling
+        deadline = time.time() + 10.0
+        while self.proc is not None and time.time() < deadline and self.proc.poll() is None:
+            self.file.flush()
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.05)
+        self.start_offset = os.path.getsize(self.file.name)
+        self.end_offset = None
         return self
+
+    def mark_start(self) -> None:
+        """Samples from here on belong to the timed region."""
+        self.file.flush()
+        self.start_offset = os.path.getsize(self.file.name)
+
+    def mark_end(self) -> None:
+        """End of the timed region; waits for one more sample so that the
+        region's last interval is covered."""
+        size = os.path.getsize(self.file.name)
+        deadline = time.time() + 1.0
+        while time.time() < deadline and os.path.getsize(self.file.name) == size:
+            time.sleep(0.01)
+        self.end_offset = os.path.getsize(self.file.name)
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -179,7 +213,9 @@ class ClockSampler:
         self.file.flush()
         rows = []
         with open(self.file.name) as f:
-            for line in f:
+            f.seek(getattr(self, "start_offset", 0))
+            text = f.read() if self.end_offset is None else f.read(self.end_offset - self.start_offset)
+            for line in text.splitlines():
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) < 10:
                     continue
@@ -205,7 +241,7 @@ def _barrier(world: int) -> None:
     torch.cuda.synchronize()
 
 
-def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: bool = True) -> dict:
+def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: bool = True, sampler=None) -> dict:
     """Advance the resident state `warmup` + `steps` RK3 steps (device CFL dt,
     device run-loop control); time the `steps` with CUDA events on the
     launching stream, and each stage launch separately."""
@@ -236,6 +272,8 @@ def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: b
     for _ in range(warmup):
         one_step()
     _barrier(world)
+    if sampler is not None:
+        sampler.mark_start()
     evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)] for _ in range(steps)]
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
@@ -243,6 +281,8 @@ def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: b
         one_step(evs[i] if stage_events else None)
     stop.record(stream)
     _barrier(world)
+    if sampler is not None:
+        sampler.mark_end()
     total_ms = start.elapsed_time(stop)
     stage_ms = [sum(evs[i][k][0].elapsed_time(evs[i][k][1]) for i in range(steps)) for k in range(3)]
     c = solver._read(ws.control, _native.CfdControl)
@@ -301,7 +341,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
             bus = str(getattr(props, "pci_bus_id", "") or "")
             sampler = ClockSampler(bus)
             with sampler:
-                r = timed_steps(solver, steps, warmup, world)
+                r = timed_steps(solver, steps, warmup, world, sampler=sampler)
             r["clocks"] = sampler.summary()
         else:
             r = timed_steps(solver, steps, warmup, world)
@@ -345,8 +385,12 @@ def run_ours(args, rank: int, world: int) -> dict | None:
             "ms_per_step": tot[name] / steps,
             "stage_ms": [round(1e3 * s, 4) for s in stage_s],
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_element_step": sum(sb)},
+                         "frac": round(achieved / peak, 4),
+                         "traffic": round(sum(NCU_BYTES_PER_ELEMENT[name]) * k / 3),
+                         "traffic_note": "bytes per stage launch (mean of the 3 launches of a step), ncu at "
+                                         "K=524,288 scaled to this K; algorithmic bytes per launch "
+                                         f"{round(sum(sb) * k / 3)}",
+                         "peak_source": peak_kind, "algorithmic_bytes_per_element_step": sum(sb)},
         }
     l1 = l1_density(fp32, results["fp32_mixed"]["state"], results["fp64"]["state"])
     state_bytes = q0.numel() * 8
@@ -503,6 +547,63 @@ def run_adjoint(args) -> dict:
     }
 
 
+def run_precision(args) -> dict:
+    """The precision study: the Sod tube on 2000x200 quads x 2 (K = 800,000),
+    hllc/van_leer, to t = 0.2, in the FP32-mixed and the plain FP64 form
+    (the FP64 GPU run is the reference: the CPU oracle would take weeks).
+    Reports the L1 / Linf density difference between the two final states,
+    each form's L1 errors against the exact solution, the shock and contact
+    positions from column-averaged density, and the mass / energy
+    conservation defects against the time-integrated boundary fluxes."""
+    import torch
+
+    from cfd_demo_b200 import sod_shock_tube
+    from cfd_demo_b200.cases import SOD_DISCONTINUITY, SOD_GAMMA, SOD_LEFT, SOD_RIGHT
+    from cfd_demo_b200.verification import ExactRiemann, column_density, front_position, l1_errors
+
+    torch.cuda.set_device(0)
+    nx, ny = args.precision_nx, args.precision_nx // 10
+    case = sod_shock_tube(nx, ny, flux="hllc", limiter="van_leer", precision="fp64")
+    solvers = {"fp64": case.solver, "fp32_mixed": case.solver.with_precision("fp32_mixed")}
+    exact = ExactRiemann((SOD_LEFT[0], SOD_LEFT[1], SOD_LEFT[3]), (SOD_RIGHT[0], SOD_RIGHT[1], SOD_RIGHT[3]),
+                         SOD_GAMMA, SOD_DISCONTINUITY)
+    t_end = case.final_time
+    waves = exact.wave_positions(t_end)
+    out, states = {}, {}
+    for name, solver in solvers.items():
+        initial = solver.integrate(case.initial_state)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = solver.run(case.initial_state, t_end)
+        wall = time.perf_counter() - t0
+        q = torch.from_numpy(res.state).cuda()
+        states[name] = q
+        cols, faces = column_density(q, solver.mesh, nx)
+        defect = solver.integrate(res.state) - initial + res.boundary_flux_integral
+        out[name] = {
+            "steps": res.steps, "rejected": res.rejected_steps, "wall_s": wall,
+            "dof_steps_per_s": res.steps * solver.mesh.num_elements * NP_NODES / wall,
+            "l1_vs_exact": l1_errors(q, solver.mesh, exact, res.time, SOD_GAMMA, n=args.precision_quad),
+            "shock_x": front_position(cols, faces, (waves["shock"] - 0.05, waves["shock"] + 0.05)),
+            "contact_x": front_position(cols, faces, (waves["contact"] - 0.05, waves["contact"] + 0.05)),
+            "mass_defect": float(defect[0]), "energy_defect": float(defect[3]),
+            "max_troubled_cells": res.max_troubled_cells, "min_density": res.min_density,
+            "min_pressure": res.min_pressure,
+        }
+    d = (states["fp32_mixed"][..., 0] - states["fp64"][..., 0]).abs()
+    w = torch.as_tensor(case.solver.reference.cell_weights, device=d.device, dtype=d.dtype)
+    l1 = float(torch.einsum("n,nk->", w, d) / (w.sum() * d.shape[1]))  # elements have equal area
+    return {
+        "metric": "precision study: FP32-mixed vs FP64 on the Sod tube", "unit": "density difference",
+        "config": {"workload": f"Sod tube {nx}x{ny} quads x 2 (K={case.solver.mesh.num_elements}), hllc/van_leer, "
+                               f"t={t_end}", "quadrature": f"{args.precision_quad}x{args.precision_quad} "
+                               "collapsed Gauss per (sub-)triangle, elements cut at the exact waves"},
+        "l1_rho_fp32_vs_fp64": l1, "linf_rho_fp32_vs_fp64": float(d.max()),
+        "exact_waves": waves, "fp64": out["fp64"], "fp32_mixed": out["fp32_mixed"],
+        "fp32_over_fp64_dof_steps": out["fp32_mixed"]["dof_steps_per_s"] / out["fp64"]["dof_steps_per_s"],
+    }
+
+
 def run_reference(args) -> dict:
     """The reference arm: the CPU oracle (NumPy restatement of the reference's
     own algorithm; JAX is not installed) on the host cores."""
@@ -532,7 +633,9 @@ def main() -> None:
     ap.add_argument("--cpu-baseline-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="stage-kernel variant (default: autotuned)")
-    ap.add_argument("--workload", choices=["microbenchmark", "batch", "adjoint"], default="microbenchmark")
+    ap.add_argument("--workload", choices=["microbenchmark", "batch", "adjoint", "precision"], default="microbenchmark")
+    ap.add_argument("--precision-nx", type=int, default=2000)
+    ap.add_argument("--precision-quad", type=int, default=6)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing of the default line")
     ap.add_argument("--batch-count", type=int, default=256)
@@ -553,6 +656,10 @@ def main() -> None:
     if args.workload == "adjoint":
         if rank == 0:
             print(json.dumps(run_adjoint(args)), flush=True)
+        return
+    if args.workload == "precision":
+        if rank == 0:
+            print(json.dumps(run_precision(args)), flush=True)
         return
 
     if args.impl == "reference":

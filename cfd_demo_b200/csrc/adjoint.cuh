@@ -171,6 +171,8 @@ struct AdjParams {
   int accumulate_src;  // 1: src_bar += ..., 0: src_bar = ...
   int limited;         // troubled-cell limiter active
   int hold_theta;      // 1: pressure-scaling theta constant (jax.grad semantics)
+  int* list;           // elements that need the full limiter replay [ld]
+  int* count;          // their number
 };
 
 __device__ __forceinline__ int element_instance(const CfdMesh& m, int e) { return m.instance ? m.instance[e] : 0; }
@@ -198,30 +200,23 @@ __device__ __forceinline__ R phi_grad(R r) {
   return R(0);
 }
 
-// qt_bar = Lambda'(qt)^T g for one element, plus the adjoints of the three
-// neighbour / ghost averages it read (gathered by adj_limit_gather_kernel).
+// Replays limit_kernel's decisions for element e (limiting.py:128-151):
+// the averages a, the positivity target, the scaled neighbour differences and
+// whether the element was troubled or needed the positivity limiter.
 template <typename R, int PHI>
-__global__ void __launch_bounds__(128) adj_limit_kernel(const AdjParams P) {
+__device__ __forceinline__ void adj_limit_decide(const AdjParams& P, int e, double a[4], double& eps, double& pt,
+                                                 R scaled[3][4], bool& troubled, bool& need_pos) {
   const CfdMesh& m = P.m;
   const int ld = m.ld;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.num_elements || element_instance(m, e) < 0) return;
   const R* __restrict__ qt = (const R*)P.qt;
-  const R* __restrict__ g = (const R*)P.g;
-  R* __restrict__ qtb = (R*)P.qtb;
-  R* __restrict__ nab = (R*)P.nab;
   const double gm1 = P.gamma - 1.0;
-  double a[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) a[c] = P.avg[c * ld + e];
   const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
-  const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
-  const double pt = pressure_target<R>(eps, pa, a[3], gm1);
+  eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
+  pt = pressure_target<R>(eps, pa, a[3], gm1);
   const int finfo = m.face_info[e];
-
-  // --- replay the detection exactly as limit_kernel does (limiting.py:128-151)
-  bool troubled = false;
-  R scaled[3][4];
+  troubled = false;
   if (PHI != LIM_UNLIMITED) {
     const double det_tol = sizeof(R) == 8 ? DETECTION_TOLERANCE : DETECTION_TOLERANCE_FP32;
     R dif[3][4];
@@ -269,16 +264,54 @@ __global__ void __launch_bounds__(128) adj_limit_kernel(const AdjParams P) {
         troubled |= (double)ex > xmul(det_tol, fabs(a[c]));
       }
   }
-  const bool need_pos = (P.aux[e] < eps) || (P.aux[ld + e] < pt);
-  if (!troubled && !need_pos) {  // the limiters left the element as it was
-#pragma unroll 1
-    for (int k = 0; k < 4 * NP; ++k) qtb[k * ld + e] = g[k * ld + e];
-    if (PHI != LIM_UNLIMITED) {
-#pragma unroll 1
-      for (int k = 0; k < 12; ++k) nab[k * ld + e] = R(0);
-    }
+  need_pos = (P.aux[e] < eps) || (P.aux[ld + e] < pt);
+}
+
+// Light pass over every element: where the limiters left the element as it
+// was, qt_bar = g and the neighbour-average adjoints are zero; the others
+// (troubled or positivity-scaled, a small minority) are listed for
+// adj_limit_heavy_kernel.
+template <typename R, int PHI>
+__global__ void __launch_bounds__(128) adj_limit_scan_kernel(const AdjParams P) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.num_elements || element_instance(m, e) < 0) return;
+  double a[4], eps, pt;
+  R scaled[3][4];
+  bool troubled, need_pos;
+  adj_limit_decide<R, PHI>(P, e, a, eps, pt, scaled, troubled, need_pos);
+  if (troubled || need_pos) {
+    P.list[atomicAdd(P.count, 1)] = e;
     return;
   }
+  const R* __restrict__ g = (const R*)P.g;
+  R* __restrict__ qtb = (R*)P.qtb;
+#pragma unroll 4
+  for (int k = 0; k < 4 * NP; ++k) qtb[k * ld + e] = g[k * ld + e];
+  if (PHI != LIM_UNLIMITED) {
+    R* __restrict__ nab = (R*)P.nab;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) nab[k * ld + e] = R(0);
+  }
+}
+
+// qt_bar = Lambda'(qt)^T g for one listed element, plus the adjoints of the
+// three neighbour / ghost averages it read (gathered by adj_lift_kernel).
+template <typename R, int PHI>
+__device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
+  const CfdMesh& m = P.m;
+  const int ld = m.ld;
+  const R* __restrict__ qt = (const R*)P.qt;
+  const R* __restrict__ g = (const R*)P.g;
+  R* __restrict__ qtb = (R*)P.qtb;
+  R* __restrict__ nab = (R*)P.nab;
+  const double gm1 = P.gamma - 1.0;
+  const int finfo = m.face_info[e];
+  double a[4], eps, pt;
+  R scaled[3][4];
+  bool troubled, need_pos;
+  adj_limit_decide<R, PHI>(P, e, a, eps, pt, scaled, troubled, need_pos);
 
   R s[NP][4];
 #pragma unroll
@@ -549,95 +582,112 @@ __global__ void __launch_bounds__(128) adj_limit_kernel(const AdjParams P) {
   }
 }
 
-// adds the neighbours' adjoints of this element's average to qt_bar
-template <typename R>
-__global__ void __launch_bounds__(128) adj_limit_gather_kernel(const AdjParams P) {
-  const CfdMesh& m = P.m;
-  const int ld = m.ld;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.num_elements || element_instance(m, e) < 0) return;
-  const R* __restrict__ nab = (const R*)P.nab;
-  R* __restrict__ qtb = (R*)P.qtb;
-  const int finfo = m.face_info[e];
-  R ab[4] = {R(0), R(0), R(0), R(0)};
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    const int info = (finfo >> (8 * f)) & 0xff;
-    if ((info & 3) != CFD_FACE_INTERIOR) continue;
-    const int nb = m.neighbor[f * ld + e];
-    const int nf = (info >> 2) & 3;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) ab[c] += nab[(nf * 4 + c) * ld + nb];
-  }
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    if (ab[c] == R(0)) continue;
-#pragma unroll
-    for (int i = 0; i < NP; ++i) qtb[(c * NP + i) * ld + e] += (R)tab::AVG_W[i] * ab[c];
-  }
+// the listed elements, grid-stride
+template <typename R, int PHI>
+__global__ void __launch_bounds__(64) adj_limit_heavy_kernel(const AdjParams P) {
+  const int n = *P.count;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    adj_limit_element<R, PHI>(P, P.list[t]);
 }
 
-// surface pass A: w = b dt Fscale LIFT^T qt_bar at the 15 face nodes
+// surface pass A: w = b dt Fscale LIFT^T qt_bar at the 15 face nodes; one
+// thread per (element, conserved variable). With the troubled-cell limiter it
+// first gathers the neighbours' adjoints of the element's average into
+// qt_bar (the adjoints the heavy limiter pass wrote for its neighbour faces).
 template <typename R>
-__global__ void __launch_bounds__(128) adj_rhs_a_kernel(const AdjParams P) {
+__global__ void __launch_bounds__(128) adj_lift_kernel(const AdjParams P) {
   const CfdMesh& m = P.m;
   const int ld = m.ld;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
   if (e >= m.num_elements) return;
   const int inst = element_instance(m, e);
   if (inst < 0) return;
-  const R* __restrict__ v = (const R*)P.qtb;
+  R* __restrict__ v = (R*)P.qtb;
   R* __restrict__ w = (R*)P.w;
   const R scale = (R)(P.b * P.dt[inst]);
   R fs[3];
 #pragma unroll
   for (int f = 0; f < 3; ++f) fs[f] = scale * (R)m.face_geo[(3 * f + 2) * ld + e];
-#pragma unroll 1
-  for (int c = 0; c < 4; ++c) {
-    R vi[NP];
+  R vi[NP];
 #pragma unroll
-    for (int i = 0; i < NP; ++i) vi[i] = v[(c * NP + i) * ld + e];
+  for (int i = 0; i < NP; ++i) vi[i] = v[(c * NP + i) * ld + e];
+  if (P.limited) {
+    // the neighbours' adjoints of this element's average (they read it in
+    // their troubled-cell tests): qt_bar += AVG_W * sum, written back for
+    // the node pass
+    const int finfo = m.face_info[e];
+    const R* __restrict__ nab = (const R*)P.nab;
+    R ab = R(0);
 #pragma unroll
-    for (int col = 0; col < 3 * NFP; ++col) {
-      R t = R(0);
-#pragma unroll
-      for (int i = 0; i < NP; ++i) t = fma((R)tab::LIFT[i][col], vi[i], t);
-      w[(c * NP + col) * ld + e] = fs[col / NFP] * t;
+    for (int f = 0; f < 3; ++f) {
+      const int info = (finfo >> (8 * f)) & 0xff;
+      if ((info & 3) == CFD_FACE_INTERIOR) ab += nab[(((info >> 2) & 3) * 4 + c) * ld + m.neighbor[f * ld + e]];
     }
+    if (ab != R(0)) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        vi[i] += (R)tab::AVG_W[i] * ab;
+        v[(c * NP + i) * ld + e] = vi[i];
+      }
+    }
+  }
+#pragma unroll
+  for (int col = 0; col < 3 * NFP; ++col) {
+    R t = R(0);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) t = fma((R)tab::LIFT[i][col], vi[i], t);
+    w[(c * NP + col) * ld + e] = fs[col / NFP] * t;
   }
 }
 
-// pass B: the adjoints of the stage input (volume + surface) and of the base state
+// pass B: the adjoints of the stage input (volume + surface) and of the base
+// state. One thread per (element, node j): a block covers ADJ_EPB elements x
+// 15 nodes (threadIdx.x = element, threadIdx.y = node, so a warp holds one
+// node of 32 elements: coalesced, and uniform in the node). The block's
+// qt_bar tile is staged in shared memory. Node j's thread owns every output
+// at node j: the volume term at j and the surface terms of the face slots
+// that meet at j (corner nodes lie on two faces).
+constexpr int ADJ_EPB = 32;
+
 template <typename R, int FLUX>
-__global__ void __launch_bounds__(128) adj_rhs_b_kernel(const AdjParams P) {
+__global__ void __launch_bounds__(ADJ_EPB * NP) adj_rhs_node_kernel(const AdjParams P) {
+  __shared__ R s_v[4 * NP][ADJ_EPB];
   const CfdMesh& m = P.m;
   const int ld = m.ld;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.num_elements) return;
+  const int lane = threadIdx.x, j = threadIdx.y;
+  const int e = blockIdx.x * ADJ_EPB + lane;
+  const bool in = e < m.num_elements;
+  const R* __restrict__ qtb = (const R*)P.qtb;
+#pragma unroll
+  for (int r = j; r < 4 * NP; r += NP) s_v[r][lane] = in ? qtb[r * ld + e] : R(0);
+  __syncthreads();
+  if (!in) return;
   const int inst = element_instance(m, e);
   if (inst < 0) return;
   const R* __restrict__ qs = (const R*)P.qs;
-  const R* __restrict__ qtb = (const R*)P.qtb;
   const R* __restrict__ w = (const R*)P.w;
   R* __restrict__ sb = (R*)P.src_bar;
   R* __restrict__ bb = (R*)P.base_bar;
   const R gamma = (R)P.gamma, gm1 = gamma - R(1);
   const R scale = (R)(P.b * P.dt[inst]);
-  const R rx = (R)m.metric[e], ry = (R)m.metric[ld + e], sx = (R)m.metric[2 * ld + e], sy = (R)m.metric[3 * ld + e];
   if (bb) {
-#pragma unroll 1
-    for (int k = 0; k < 4 * NP; ++k) bb[k * ld + e] += (R)P.a * qtb[k * ld + e];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bb[(c * NP + j) * ld + e] += (R)P.a * s_v[c * NP + j][lane];
   }
-  // volume
-#pragma unroll 1
-  for (int j = 0; j < NP; ++j) {
+  // volume at node j: Ft_bar_j = -sum_i Dr[i][j] v_i, Gt_bar_j likewise
+  R q[4], acc[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) q[c] = qs[(c * NP + j) * ld + e];
+  {
+    const R rx = (R)m.metric[e], ry = (R)m.metric[ld + e], sx = (R)m.metric[2 * ld + e], sy = (R)m.metric[3 * ld + e];
     R fb[4], gb[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       R sf = R(0), sg = R(0);
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
-        const R vi = qtb[(c * NP + i) * ld + e];
+        const R vi = s_v[c * NP + i][lane];
         sf = fma((R)ctab::DR[i][j], vi, sf);
         sg = fma((R)ctab::DS[i][j], vi, sg);
       }
@@ -645,35 +695,25 @@ __global__ void __launch_bounds__(128) adj_rhs_b_kernel(const AdjParams P) {
       fb[c] = rx * ftb + sx * gtb;
       gb[c] = ry * ftb + sy * gtb;
     }
-    R q[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) q[c] = qs[(c * NP + j) * ld + e];
     R jf[4], jg[4];
     normal_flux_vjp(q, R(1), R(0), gm1, fb, jf);
     normal_flux_vjp(q, R(0), R(1), gm1, gb, jg);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int idx = (c * NP + j) * ld + e;
-      const R val = (R)P.b * qtb[idx] + jf[c] + jg[c];
-      sb[idx] = P.accumulate_src ? sb[idx] + val : val;
-    }
+    for (int c = 0; c < 4; ++c) acc[c] = (R)P.b * s_v[c * NP + j][lane] + jf[c] + jg[c];
   }
-  // surface
+  // surface: the face slots (f, k) whose node is j
   const int finfo = m.face_info[e];
 #pragma unroll 1
   for (int sl = 0; sl < 3 * NFP; ++sl) {
     const int f = sl / NFP, k = sl - f * NFP;
+    if (face_node_rt(f, k) != j) continue;  // warp-uniform
     const int info = (finfo >> (8 * f)) & 0xff;
     const int kind = info & 3;
     const R nx = (R)m.face_geo[(3 * f) * ld + e], ny = (R)m.face_geo[(3 * f + 1) * ld + e];
-    const int n = face_node_rt(f, k);
-    R qm[4], qp[4], wo[4], jfm[4], contrib[4];
+    R qp[4], wo[4], jfm[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      qm[c] = qs[(c * NP + n) * ld + e];
-      wo[c] = w[(c * NP + sl) * ld + e];
-    }
-    normal_flux_vjp(qm, nx, ny, gm1, wo, jfm);
+    for (int c = 0; c < 4; ++c) wo[c] = w[(c * NP + sl) * ld + e];
+    normal_flux_vjp(q, nx, ny, gm1, wo, jfm);
     if (kind == CFD_FACE_INTERIOR) {
       const int nb = m.neighbor[f * ld + e];
       const int nf = (info >> 2) & 3;
@@ -685,40 +725,43 @@ __global__ void __launch_bounds__(128) adj_rhs_b_kernel(const AdjParams P) {
         qp[c] = qs[(c * NP + pn) * ld + nb];
         wd[c] = w[(c * NP + nf * NFP + kk) * ld + nb] - wo[c];
       }
-      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wd, 0, jm);
+      iflux_vjp<R, FLUX>(q, qp, nx, ny, gamma, wd, 0, jm);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) contrib[c] = jfm[c] + jm[c];
+      for (int c = 0; c < 4; ++c) acc[c] += jfm[c] + jm[c];
     } else if (kind == CFD_FACE_SLIP_WALL) {
-      const R mn = qm[1] * nx + qm[2] * ny;
-      qp[0] = qm[0];
-      qp[1] = qm[1] - R(2) * mn * nx;
-      qp[2] = qm[2] - R(2) * mn * ny;
-      qp[3] = qm[3];
+      const R mn = q[1] * nx + q[2] * ny;
+      qp[0] = q[0];
+      qp[1] = q[1] - R(2) * mn * nx;
+      qp[2] = q[2] - R(2) * mn * ny;
+      qp[3] = q[3];
       R jm[4], jp[4];
-      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 0, jm);
-      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 1, jp);
+      iflux_vjp<R, FLUX>(q, qp, nx, ny, gamma, wo, 0, jm);
+      iflux_vjp<R, FLUX>(q, qp, nx, ny, gamma, wo, 1, jp);
       // q+ = M q- with M = M^T (the normal momentum reversed)
       const R dm = jp[1] * nx + jp[2] * ny;
-      contrib[0] = jfm[0] - jm[0] - jp[0];
-      contrib[1] = jfm[1] - jm[1] - (jp[1] - R(2) * dm * nx);
-      contrib[2] = jfm[2] - jm[2] - (jp[2] - R(2) * dm * ny);
-      contrib[3] = jfm[3] - jm[3] - jp[3];
+      acc[0] += jfm[0] - jm[0] - jp[0];
+      acc[1] += jfm[1] - jm[1] - (jp[1] - R(2) * dm * nx);
+      acc[2] += jfm[2] - jm[2] - (jp[2] - R(2) * dm * ny);
+      acc[3] += jfm[3] - jm[3] - jp[3];
     } else {
       const int row = m.neighbor[f * ld + e];
 #pragma unroll
       for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
       R jm[4];
-      iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 0, jm);
+      iflux_vjp<R, FLUX>(q, qp, nx, ny, gamma, wo, 0, jm);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) contrib[c] = jfm[c] - jm[c];
+      for (int c = 0; c < 4; ++c) acc[c] += jfm[c] - jm[c];
       if (P.bc_bar) {
         R jp[4];
-        iflux_vjp<R, FLUX>(qm, qp, nx, ny, gamma, wo, 1, jp);
+        iflux_vjp<R, FLUX>(q, qp, nx, ny, gamma, wo, 1, jp);
 #pragma unroll
         for (int c = 0; c < 4; ++c) atomicAdd(&P.bc_bar[row * 4 + c], -(double)jp[c]);
       }
     }
+  }
 #pragma unroll
-    for (int c = 0; c < 4; ++c) sb[(c * NP + n) * ld + e] += contrib[c];
+  for (int c = 0; c < 4; ++c) {
+    const int idx = (c * NP + j) * ld + e;
+    sb[idx] = P.accumulate_src ? sb[idx] + acc[c] : acc[c];
   }
 }

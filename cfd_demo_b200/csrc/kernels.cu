@@ -1259,26 +1259,37 @@ double* tape_aux(void* tape, int ld, int precision, int k) {
   return (double*)((char*)tape + 5 * state_bytes(ld, precision)) + (size_t)12 * ld + (size_t)(k - 1) * 2 * ld;
 }
 // adjoint scratch: qt_bar, face-node adjoints w, neighbour-average adjoints,
-// and the adjoints of q1 and q2 (60 + 60 + 12 + 60 + 60 rows)
-size_t adjoint_work_bytes(int ld, int precision) { return (size_t)252 * ld * (precision == CFD_FP64 ? 8 : 4); }
+// the adjoints of q1 and q2 (60 + 60 + 12 + 60 + 60 rows of the solver
+// precision), the list of elements for the full limiter replay (ld ints) and
+// its counter
+size_t adjoint_reals_bytes(int ld, int precision) { return (size_t)252 * ld * (precision == CFD_FP64 ? 8 : 4); }
+size_t adjoint_work_bytes(int ld, int precision) { return adjoint_reals_bytes(ld, precision) + (size_t)4 * ld + 256; }
 
+template <typename R, int PHI>
+void launch_adj_limit_phi(const AdjParams& p, int n, cudaStream_t st) {
+  adj_limit_scan_kernel<R, PHI><<<blocks_for(n, 128), 128, 0, st>>>(p);
+  // the listed elements are a small minority: a grid of a few blocks per SM
+  const unsigned hb = (unsigned)(blocks_for(n, 64) < 4 * 148 ? blocks_for(n, 64) : 4 * 148);
+  adj_limit_heavy_kernel<R, PHI><<<hb, 64, 0, st>>>(p);
+}
 template <typename R>
-void launch_adj_limit(const AdjParams& p, int lim, unsigned g, cudaStream_t st) {
+void launch_adj_limit(const AdjParams& p, int lim, int n, cudaStream_t st) {
   switch (lim) {
-    case 0: adj_limit_kernel<R, 0><<<g, 128, 0, st>>>(p); break;
-    case 1: adj_limit_kernel<R, 1><<<g, 128, 0, st>>>(p); break;
-    case 2: adj_limit_kernel<R, 2><<<g, 128, 0, st>>>(p); break;
-    case 3: adj_limit_kernel<R, 3><<<g, 128, 0, st>>>(p); break;
-    default: adj_limit_kernel<R, 4><<<g, 128, 0, st>>>(p); break;
+    case 0: launch_adj_limit_phi<R, 0>(p, n, st); break;
+    case 1: launch_adj_limit_phi<R, 1>(p, n, st); break;
+    case 2: launch_adj_limit_phi<R, 2>(p, n, st); break;
+    case 3: launch_adj_limit_phi<R, 3>(p, n, st); break;
+    default: launch_adj_limit_phi<R, 4>(p, n, st); break;
   }
 }
 template <typename R>
-void launch_adj_rhs(const AdjParams& p, int flux, unsigned g, cudaStream_t st) {
-  adj_rhs_a_kernel<R><<<g, 128, 0, st>>>(p);
+void launch_adj_rhs(const AdjParams& p, int flux, int n, cudaStream_t st) {
+  adj_lift_kernel<R><<<dim3(blocks_for(n, 128), 4), 128, 0, st>>>(p);
+  const dim3 grid(blocks_for(n, ADJ_EPB)), block(ADJ_EPB, NP);
   switch (flux) {
-    case 0: adj_rhs_b_kernel<R, 0><<<g, 128, 0, st>>>(p); break;
-    case 1: adj_rhs_b_kernel<R, 1><<<g, 128, 0, st>>>(p); break;
-    default: adj_rhs_b_kernel<R, 2><<<g, 128, 0, st>>>(p); break;
+    case 0: adj_rhs_node_kernel<R, 0><<<grid, block, 0, st>>>(p); break;
+    case 1: adj_rhs_node_kernel<R, 1><<<grid, block, 0, st>>>(p); break;
+    default: adj_rhs_node_kernel<R, 2><<<grid, block, 0, st>>>(p); break;
   }
 }
 }  // namespace
@@ -1367,9 +1378,11 @@ int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape,
   void* nab = wk + 2 * sb;
   void* b1 = wk + 2 * sb + (size_t)12 * ld * es;  // adjoint of q1
   void* b2 = (char*)b1 + sb;                      // adjoint of q2
+  int* list = (int*)(wk + adjoint_reals_bytes(ld, prec));
+  int* count = (int*)(wk + adjoint_reals_bytes(ld, prec) + (size_t)4 * ld);
   void* tp = const_cast<void*>(tape);
   if (cudaMemsetAsync(g_in, 0, sb, st) != cudaSuccess) return check_launch("cfd_rk3_step_adjoint: memset");
-  const unsigned g = blocks_for(s->mesh.num_elements, 128);
+  const int n = s->mesh.num_elements;
   static const double A[4] = {0.0, 0.0, 0.75, 1.0 / 3.0}, B[4] = {0.0, 1.0, 0.25, 2.0 / 3.0};
   for (int k = 3; k >= 1; --k) {
     AdjParams p;
@@ -1393,14 +1406,15 @@ int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape,
     p.accumulate_src = k == 1;
     p.limited = s->limiter != CFD_LIMITER_UNLIMITED;
     p.hold_theta = (flags & CFD_ADJ_HOLD_THETA) != 0;
+    p.list = list;
+    p.count = count;
+    if (cudaMemsetAsync(count, 0, sizeof(int), st) != cudaSuccess) return check_launch("cfd_rk3_step_adjoint: memset");
     if (prec == CFD_FP64) {
-      launch_adj_limit<double>(p, s->limiter, g, st);
-      if (p.limited) adj_limit_gather_kernel<double><<<g, 128, 0, st>>>(p);
-      launch_adj_rhs<double>(p, s->flux, g, st);
+      launch_adj_limit<double>(p, s->limiter, n, st);
+      launch_adj_rhs<double>(p, s->flux, n, st);
     } else {
-      launch_adj_limit<float>(p, s->limiter, g, st);
-      if (p.limited) adj_limit_gather_kernel<float><<<g, 128, 0, st>>>(p);
-      launch_adj_rhs<float>(p, s->flux, g, st);
+      launch_adj_limit<float>(p, s->limiter, n, st);
+      launch_adj_rhs<float>(p, s->flux, n, st);
     }
   }
   return check_launch("cfd_rk3_step_adjoint");

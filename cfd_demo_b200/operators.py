@@ -23,6 +23,7 @@ and neighbour indices are then global.
 from __future__ import annotations
 
 from dataclasses import dataclass, field
+from typing import NamedTuple
 
 import numpy as np
 
@@ -114,6 +115,42 @@ def check_face_pairing(mesh: TriangleMesh, connectivity: MeshConnectivity, refer
             dist = np.hypot(x[fn[f, k], el] - x[pn, nb], y[fn[f, k], el] - y[pn, nb])
             if np.any(dist > relative_tolerance * lengths[el, f]):
                 raise ValueError("Neighboring face nodes do not coincide; the mesh is not conforming.")
+
+
+class LimiterOperators(NamedTuple):
+    """Host (NumPy) copies of the limiter tables under the reference's field
+    names (limiting.py:34-48, built by build_limiter_operators, :97-121); face
+    arrays are (3, K). The kernels read the same data from the packed
+    CfdMesh tables."""
+
+    average_weights: np.ndarray  # (Np,)
+    midpoint_nodes: np.ndarray  # (3,)
+    p1_midpoint: np.ndarray  # (3, Np)
+    linear_basis: np.ndarray  # (Np, 3)
+    neighbor: np.ndarray  # (3, K): neighbour element, or the element itself on boundaries
+    neighbor_kind: np.ndarray  # (3, K): 0 interior, SLIP_WALL or FIXED_STATE
+    normal_x: np.ndarray  # (3, K)
+    normal_y: np.ndarray  # (3, K)
+    fixed_state: np.ndarray  # (3, K, 4)
+    alpha: np.ndarray  # (3, K)
+    beta: np.ndarray  # (3, K)
+    partner_face: np.ndarray  # (3, K)
+
+
+def limiter_operators(connectivity: MeshConnectivity, geometry, reference, kind: np.ndarray,
+                      state: np.ndarray) -> LimiterOperators:
+    alpha, beta, partner = neighbor_coefficients(connectivity, geometry)
+    k = connectivity.neighbor_element.shape[0]
+    own = np.broadcast_to(np.arange(k)[:, None], (k, 3))
+    nbr = np.where(connectivity.neighbor_element >= 0, connectivity.neighbor_element, own)
+    w = reference.cell_weights
+    return LimiterOperators(
+        average_weights=w / w.sum(), midpoint_nodes=np.asarray(reference.face_midpoint_nodes),
+        p1_midpoint=np.asarray(reference.p1_midpoint), linear_basis=np.asarray(reference.linear_midpoint_basis),
+        neighbor=nbr.T.copy(), neighbor_kind=np.asarray(kind).T.copy(),
+        normal_x=geometry.normal[:, :, 0].T.copy(), normal_y=geometry.normal[:, :, 1].T.copy(),
+        fixed_state=np.transpose(state, (1, 0, 2)).copy(), alpha=alpha.T.copy(), beta=beta.T.copy(),
+        partner_face=np.asarray(partner).T.copy())
 
 
 @dataclass

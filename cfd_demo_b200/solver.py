@@ -30,7 +30,7 @@ from .euler import NUM_VARIABLES
 from .fluxes import FLUX_IDS, get_interface_flux
 from .limiters import LIMITER_IDS, get_limiter_function
 from .mesh import TriangleMesh, build_connectivity, element_geometry, node_coordinates
-from .operators import DeviceTables, host_tables, resolve_boundary_conditions
+from .operators import DeviceTables, LimiterOperators, host_tables, limiter_operators, resolve_boundary_conditions
 from .reference_element import DEGREE, build_reference_triangle
 
 DEFAULT_CFL = 0.5  # time_integration.py:18
@@ -200,6 +200,17 @@ class EulerSolver:
     @property
     def state_shape(self) -> tuple[int, int, int]:
         return (self.reference.num_nodes, self.mesh.num_elements, NUM_VARIABLES)
+
+    @property
+    def limiter_operators(self) -> LimiterOperators:
+        """The limiter tables under the reference's names (solver.py:110 of
+        CFD-demo builds them as a JAX pytree); host NumPy arrays here."""
+        ops = getattr(self, "_limiter_operators", None)
+        if ops is None:
+            kind, state = resolve_boundary_conditions(self.connectivity, self.boundary_conditions)
+            ops = limiter_operators(self.connectivity, self.geometry, self.reference, kind, state)
+            self._limiter_operators = ops
+        return ops
 
     def node_coordinates(self) -> tuple[np.ndarray, np.ndarray]:
         """Physical node coordinates (x, y), each of shape (Np, K)."""

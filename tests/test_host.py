@@ -101,6 +101,33 @@ def test_cockburn_shu_coefficients_match_oracle():
     assert np.array_equal(a.T, s.alpha) and np.array_equal(b.T, s.beta) and np.array_equal(p.T, s.partner_face)
 
 
+def test_limiter_operators_match_oracle_tables():
+    """EulerSolver.limiter_operators (the reference's LimiterOperators fields)
+    against the oracle's limiter tables."""
+    from cfd_demo_b200 import mesh as pm
+    from cfd_demo_b200.boundary import FixedState as PFixed, SlipWall as PSlip
+    from cfd_demo_b200.operators import limiter_operators, resolve_boundary_conditions
+    from cfd_demo_b200.reference_element import build_reference_triangle
+    from oracle.physics import FixedState, SlipWall
+
+    om = oracle.mesh.perturbed_mesh(6, 4, 0.2, 2)
+    st = (1.0, 0.1, 0.0, 2.5)
+    s = oracle.OracleSolver(om, {"left": FixedState(st), "right": FixedState(st), "bottom": SlipWall(),
+                                 "top": SlipWall()}, flux="rusanov", limiter="minmod", gamma=1.4)
+    m = pm.TriangleMesh(om.vertices, om.elements, om.boundary_edges)
+    conn, geo = pm.build_connectivity(m), pm.element_geometry(m)
+    kind, state = resolve_boundary_conditions(conn, {"left": PFixed(st), "right": PFixed(st), "bottom": PSlip(),
+                                                     "top": PSlip()})
+    lo = limiter_operators(conn, geo, build_reference_triangle(4), kind, state)
+    assert np.array_equal(lo.average_weights, s.avg_weights)
+    assert np.array_equal(lo.neighbor, s.nbr3) and np.array_equal(lo.neighbor_kind, s.kind3)
+    assert np.array_equal(lo.normal_x, s.nx3) and np.array_equal(lo.normal_y, s.ny3)
+    assert np.array_equal(lo.fixed_state, s.fixed3)
+    assert np.array_equal(lo.alpha, s.alpha) and np.array_equal(lo.beta, s.beta)
+    assert np.array_equal(lo.partner_face, s.partner_face)
+    assert lo.p1_midpoint.shape == (3, 15) and lo.linear_basis.shape == (15, 3) and lo.midpoint_nodes.shape == (3,)
+
+
 def test_host_tables_layout():
     from cfd_demo_b200 import FixedState, SlipWall
     from cfd_demo_b200 import mesh as pm
@@ -209,7 +236,7 @@ def test_adjoint_buffer_sizes():
     # tape: five stage states (before / after limiting) + 3 x (4 averages + 2 minima) doubles
     assert lib.cfd_tape_bytes(ld, _native.CFD_FP64) == 5 * 60 * ld * 8 + 18 * ld * 8
     assert lib.cfd_tape_bytes(ld, _native.CFD_FP32_MIXED) == 5 * 60 * ld * 4 + 18 * ld * 8
-    assert lib.cfd_adjoint_work_bytes(ld, _native.CFD_FP64) == 252 * ld * 8
+    assert lib.cfd_adjoint_work_bytes(ld, _native.CFD_FP64) == 252 * ld * 8 + 4 * ld + 256
     assert lib.cfd_tape_bytes(0, _native.CFD_FP64) == -1
     assert lib.cfd_adjoint_work_bytes(ld, 9) == -1
 
