@@ -220,11 +220,14 @@ class ClockSampler:
                 if len(parts) < 10:
                     continue
                 bus = parts[1].lower()
-                if self.bus_id and not (bus.endswith(self.bus_id[-12:]) or self.bus_id.endswith(bus[-12:])):
+                if self.bus_id and not bus.startswith(self.bus_id):
                     continue
                 rows.append(parts)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+            with open(self.file.name) as f:
+                head = f.read(300).strip().splitlines()
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"],
+                    "bus_id": self.bus_id, "first_line": head[0] if head else None}
         sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({n for r in rows for n, v in zip(names, r[6:10]) if v.strip().lower() == "active"})
@@ -233,6 +236,18 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- GPU timing ---
+def max_over_ranks(values, world: int, device) -> list:
+    """Element-wise maximum of per-rank timings (the replicas' whole-job time
+    is that of the slowest rank); identity on one rank."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def _barrier(world: int) -> None:
     import torch
 
@@ -338,7 +353,10 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         solver.begin_run(q0, math.inf)
         if name == "fp32_mixed":
             props = torch.cuda.get_device_properties(dev)
-            bus = str(getattr(props, "pci_bus_id", "") or "")
+            # nvidia-smi prints the PCI address as dddddddd:bb:dd.f
+            bus = "%08x:%02x:%02x" % (int(getattr(props, "pci_domain_id", 0) or 0),
+                                      int(getattr(props, "pci_bus_id", 0) or 0),
+                                      int(getattr(props, "pci_device_id", 0) or 0))
             sampler = ClockSampler(bus)
             with sampler:
                 r = timed_steps(solver, steps, warmup, world, sampler=sampler)
@@ -349,11 +367,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         results[name] = r
 
     # max over ranks of the timed region
-    tot = {n: results[n]["total_ms"] for n in results}
-    if world > 1:
-        t = torch.tensor([tot["fp32_mixed"], tot["fp64"]], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot = {"fp32_mixed": float(t[0]), "fp64": float(t[1])}
+    m32, m64 = max_over_ranks([results["fp32_mixed"]["total_ms"], results["fp64"]["total_ms"]], world, dev)
+    tot = {"fp32_mixed": m32, "fp64": m64}
 
     # end to end through the public API: pinned host state in, host result out
     host_q0 = q0.cpu().pin_memory()
@@ -365,10 +380,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - w0
     e2e_steps = res.steps
-    e2e_t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_s = float(e2e_t[0])
+    e2e_s = max_over_ranks([e2e_s], world, dev)[0]
 
     if rank != 0:
         return None

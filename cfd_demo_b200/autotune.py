@@ -1,11 +1,13 @@
 """Autotuner of the stage-kernel shape (elements per block, tile staging).
 
-The fused stage kernel comes in four shapes (CfdSolver.variant):
+The fused stage kernel comes in five shapes (CfdSolver.variant):
   0  tiled, 32 elements (64 threads) per block, state and geometry staged in
      shared memory, stage base read from global memory in the epilogue
   1  tiled, 32 elements per block, stage base staged in shared memory too
   2  register-only pair kernel (block size 64/128/256 threads)
   3  tiled, 64 elements (128 threads) per block
+  4  tiled, 32 elements per block, registers capped so that 10 (FP32) / 8
+     (FP64) blocks fit on an SM instead of 8 / 6
 `autotune(solver, state)` times one RK3 attempt per candidate on the solver's
 own buffers (an attempt from the same state recomputes the same step, so the
 candidates see identical work), keeps the fastest, and remembers the choice per
@@ -19,7 +21,7 @@ import math
 
 from . import _native
 
-CANDIDATES = ((0, 0), (1, 0), (3, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
+CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
 _cache: dict = {}
 
 

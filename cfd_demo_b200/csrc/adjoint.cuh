@@ -159,6 +159,7 @@ struct AdjParams {
   const void* qt;      // pre-limiting stage state (tape)
   const double* avg;   // its cell averages [4][ld] (tape)
   const double* aux;   // its nodal density / pressure minima [2][ld] (tape)
+  const double* pos;   // the positivity limiter's pressure theta and critical node [2][ld] (tape)
   const void* qs;      // stage input state
   const void* g;       // adjoint of the limited stage state
   void* qtb;           // adjoint of qt (out)
@@ -377,32 +378,10 @@ __device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) s[i][c] = (R)xadd(a[c], xmul(th1, xsub((double)s[i][c], a[c])));
   }
-  double th2 = 1.0;
-  int i2 = -1;  // the node whose bisection set th2
-#pragma unroll 1
-  for (int i = 0; i < NP; ++i) {
-    double qi[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      double v = 0.0;
-#pragma unroll
-      for (int j = 0; j < NP; ++j) v = (j == i) ? (double)s[j][c] : v;
-      qi[c] = v;
-    }
-    if (!(pressure_near(qi[0], qi[1], qi[2], qi[3], gm1, pt) < pt)) continue;
-    const double d0 = xsub(qi[0], a[0]), d1 = xsub(qi[1], a[1]), d2 = xsub(qi[2], a[2]), d3 = xsub(qi[3], a[3]);
-    double lo = 0.0, hi = 1.0;
-#pragma unroll 1
-    for (int it = 0; it < BISECTION_STEPS; ++it) {
-      const double mid = xmul(0.5, xadd(lo, hi));
-      const bool ok = pressure_x(xadd(a[0], xmul(mid, d0)), xadd(a[1], xmul(mid, d1)), xadd(a[2], xmul(mid, d2)),
-                                 xadd(a[3], xmul(mid, d3)), gm1) >= pt;
-      lo = ok ? mid : lo;
-      hi = ok ? hi : mid;
-    }
-    if (lo < th2) i2 = i;
-    th2 = jmin(th2, lo);
-  }
+  // the pressure-scaling theta and its critical node, as the forward
+  // bisection found them (limit_kernel records them in the tape)
+  double th2 = P.pos[e];
+  const int i2 = (int)P.pos[ld + e];
   if (!(th2 < 1.0)) th2 = 1.0;
 
   // --- reverse pass; y is the running adjoint of the nodal state, abar that

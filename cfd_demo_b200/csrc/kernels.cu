@@ -253,7 +253,8 @@ __device__ __forceinline__ void cell_average(const R (&q)[NP][4], double a[4]) {
 // and in the reference's operation order (limiting.py:166-200). q is the
 // element's nodal state in registers. Returns true if q changed.
 template <typename R>
-__device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], double gm1) {
+__device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], double gm1, double* theta_out = nullptr,
+                                           int* node_out = nullptr) {
   const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
   const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
   const double pt = pressure_target<R>(eps, pa, a[3], gm1);
@@ -274,6 +275,10 @@ __device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], dou
 #pragma unroll
   for (int i = 0; i < NP; ++i)
     if (pressure_near(q[i][0], q[i][1], q[i][2], q[i][3], gm1, pt) < pt) need |= 1u << i;
+  if (theta_out) {
+    *theta_out = 1.0;
+    *node_out = -1;
+  }
   if (!need) return changed;
   double theta = 1.0;
 #pragma unroll 1
@@ -298,8 +303,10 @@ __device__ __forceinline__ bool positivity(R (&q)[NP][4], const double a[4], dou
       lo = ok ? mid : lo;
       hi = ok ? hi : mid;
     }
+    if (theta_out && lo < theta) *node_out = i;
     theta = jmin(theta, lo);
   }
+  if (theta_out) *theta_out = theta;
   if (theta < 1.0) {
 #pragma unroll
     for (int i = 0; i < NP; ++i)
@@ -359,7 +366,7 @@ __device__ __forceinline__ void face_node_flux(const CfdMesh& m, const R* __rest
     for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[nb * 4 + c];
   }
   R fhat[4], fm[4];
-  interface_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+  trace_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
 #pragma unroll
   for (int c = 0; c < 4; ++c) jump[c] = fs * (fm[c] - fhat[c]);
   if (kind != CFD_FACE_INTERIOR) {
@@ -383,6 +390,8 @@ struct StageParams {
   const void* q_in;  // MODE_RHS
   void* q_out;       // MODE_RHS
   double* bflux_out; // MODE_RHS, [instances][4]
+  void* tape_src;    // optional: copy of the stage input written here (tiled kernels)
+  void* tape_dst;    // optional: second copy of the stage result (before limiting)
 };
 
 template <typename R>
@@ -404,6 +413,18 @@ __device__ __forceinline__ void select_buffers(const StageParams& P, int par, co
   }
 }
 
+// SSP-RK3 third stage q = q_n / 3 + 2 (q_2 + dt L(q_2)) / 3 with v = q_2 +
+// dt L(q_2) (time_integration.py:64-66). The plain form evaluates it as the
+// reference does. In single precision float(1/3) + float(2/3) = 1 + 3e-8,
+// which would scale the whole state by that factor every step (a steady
+// drift of mass and energy), so the FP32 form uses q_n + (2/3)(v - q_n),
+// whose weights sum to one exactly.
+template <typename R>
+__device__ __forceinline__ R stage3_combine(R b, R v) {
+  if (sizeof(R) == 8) return b * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
+  return fma((R)(2.0 / 3.0), v - b, b);
+}
+
 #include "stage_pair.cuh"
 #include "stage_tile.cuh"
 
@@ -421,6 +442,7 @@ struct LimitParams {
   const double* aux;
   CfdStageAcc* acc;       // stage mode
   int32_t* troubled_out;  // cfd_limit mode
+  double* pos_out;        // optional [2][ld]: pressure-scaling theta and its critical node
 };
 
 // Cockburn-Shu troubled-cell limiter (limiting.py:136-163) followed by the
@@ -565,7 +587,15 @@ __global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
         }
         red.tr = 1;
       }
-      positivity<R>(s, a, gm1);
+      if (P.pos_out) {
+        double th;
+        int node;
+        positivity<R>(s, a, gm1, &th, &node);
+        P.pos_out[e] = th;
+        P.pos_out[ld + e] = (double)node;
+      } else {
+        positivity<R>(s, a, gm1);
+      }
 #pragma unroll
       for (int i = 0; i < NP; ++i)
 #pragma unroll
@@ -892,7 +922,7 @@ static int validate(const CfdSolver* s) {
   if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
   if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
     return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
-  if (s->variant < 0 || s->variant > 3) return fail(CFD_E_ARG, "variant must be 0..3");
+  if (s->variant < 0 || s->variant > 4) return fail(CFD_E_ARG, "variant must be 0..4");
   if (s->variant != 2 && s->mesh.instance && s->mesh.num_instances > 1 && (s->mesh.flags & 1) == 0)
     return fail(CFD_E_ARG, "tiled stage kernels need instance ranges aligned to 64 elements (CfdMesh.flags bit 0)");
   return CFD_OK;
@@ -915,23 +945,24 @@ static void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream
   else if (flux == 1) launch_stage_bs<R, 1, MODE>(p, bs, st);
   else launch_stage_bs<R, 2, MODE>(p, bs, st);
 }
-template <typename R, int FLUX, int MODE, int EPB, bool SB>
+template <typename R, int FLUX, int MODE, int EPB, bool SB, int MINB = (sizeof(R) == 4 ? 512 : 384) / (2 * EPB)>
 static void launch_tile(const StageParams& p, cudaStream_t st) {
   using L = TileLayout<R, EPB, SB>;
   static bool configured = false;  // per instantiation: opt in to > 48 KB of dynamic shared memory
   if (!configured) {
-    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          L::BYTES);
     configured = true;
   }
   const unsigned g = blocks_for(p.m.num_elements, EPB);
-  stage_tile_kernel<R, FLUX, MODE, EPB, SB><<<g, 2 * EPB, L::BYTES, st>>>(p);
+  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB><<<g, 2 * EPB, L::BYTES, st>>>(p);
 }
 template <typename R, int FLUX, int MODE>
 static void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_t st) {
   if (variant == 2) launch_stage_bs<R, FLUX, MODE>(p, bs, st);
   else if (variant == 1) launch_tile<R, FLUX, MODE, 32, true>(p, st);
   else if (variant == 3) launch_tile<R, FLUX, MODE, 64, false>(p, st);
+  else if (variant == 4) launch_tile<R, FLUX, MODE, 32, false, sizeof(R) == 4 ? 10 : 8>(p, st);
   else launch_tile<R, FLUX, MODE, 32, false>(p, st);
 }
 template <typename R, int MODE>
@@ -1245,19 +1276,22 @@ int cfd_limiter_phi(int32_t limiter, int32_t n, const double* r, double* out, vo
 // ------------------------------------------------ fixed-size step + adjoint ---
 // Tape of one step (sizes in elements of ld): the pre-limiting stage states
 // qt1, qt2, qt3 and the limited stage states q1, q2 (60 rows each, solver
-// precision) in the order qt1 q1 qt2 q2 qt3, then the cell averages of
-// qt1..qt3 (4 rows of double each) and their nodal density / pressure minima
-// (2 rows of double each).
+// precision) in the order qt1 q1 qt2 q2 qt3, then per stage k = 1..3 nine rows
+// of double: the cell averages of qt_k (4), its nodal density / pressure
+// minima and wave speed (3), and the positivity limiter's pressure-scaling
+// theta and critical node (2, written for the elements it processed).
 namespace {
+constexpr int TAPE_ROWS_PER_STAGE = 9;
 size_t state_bytes(int ld, int precision) { return (size_t)60 * ld * (precision == CFD_FP64 ? 8 : 4); }
-size_t tape_bytes(int ld, int precision) { return 5 * state_bytes(ld, precision) + (size_t)18 * ld * 8; }
+size_t tape_bytes(int ld, int precision) {
+  return 5 * state_bytes(ld, precision) + (size_t)3 * TAPE_ROWS_PER_STAGE * ld * 8;
+}
 char* tape_state(void* tape, int ld, int precision, int slot) { return (char*)tape + slot * state_bytes(ld, precision); }
 double* tape_avg(void* tape, int ld, int precision, int k) {
-  return (double*)((char*)tape + 5 * state_bytes(ld, precision)) + (size_t)(k - 1) * 4 * ld;
+  return (double*)((char*)tape + 5 * state_bytes(ld, precision)) + (size_t)(k - 1) * TAPE_ROWS_PER_STAGE * ld;
 }
-double* tape_aux(void* tape, int ld, int precision, int k) {
-  return (double*)((char*)tape + 5 * state_bytes(ld, precision)) + (size_t)12 * ld + (size_t)(k - 1) * 2 * ld;
-}
+double* tape_aux(void* tape, int ld, int precision, int k) { return tape_avg(tape, ld, precision, k) + (size_t)4 * ld; }
+double* tape_pos(void* tape, int ld, int precision, int k) { return tape_avg(tape, ld, precision, k) + (size_t)7 * ld; }
 // adjoint scratch: qt_bar, face-node adjoints w, neighbour-average adjoints,
 // the adjoints of q1 and q2 (60 + 60 + 12 + 60 + 60 rows of the solver
 // precision), the list of elements for the full limiter replay (ld ints) and
@@ -1317,7 +1351,11 @@ int cfd_rk3_step_fixed(const CfdSolver* s, const void* q_in, void* q_out, void* 
   const int n = s->mesh.num_instances, ld = s->mesh.ld, prec = s->precision;
   fixed_control_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->control, dt, n);
   reset_acc(s, st);
-  const size_t sb = state_bytes(ld, prec);
+  // with a tape, the tiled stage kernel writes its input tile and its result
+  // into the tape as it goes (the register-only pair kernel cannot copy its
+  // input), and the averages / minima / positivity theta land there directly
+  CfdSolver sv = *s;
+  if (tape && sv.variant == 2) sv.variant = 0;
   for (int k = 1; k <= 3; ++k) {
     StageParams p;
     memset(&p, 0, sizeof(p));
@@ -1328,19 +1366,16 @@ int cfd_rk3_step_fixed(const CfdSolver* s, const void* q_in, void* q_out, void* 
     p.stage = stage;
     p.stage_idx = k;
     p.gamma = s->gamma;
-    p.avg = s->averages;
-    p.aux = s->element_aux;
+    p.avg = tape ? tape_avg(tape, ld, prec, k) : s->averages;
+    p.aux = tape ? tape_aux(tape, ld, prec, k) : s->element_aux;
     p.acc = s->acc;
+    if (tape) {
+      p.tape_dst = tape_state(tape, ld, prec, 2 * (k - 1));
+      p.tape_src = k >= 2 ? tape_state(tape, ld, prec, 2 * k - 3) : nullptr;
+    }
     // the limited path for every limiter: positivity runs in limit_kernel on
     // the stored stage state, so the tape sees the state before limiting
-    launch_stage(s, p, MODE_LIMITED, st);
-    void* dst = k == 2 ? stage : q_out;
-    if (tape) {
-      if (cudaMemcpyAsync(tape_state(tape, ld, prec, 2 * (k - 1)), dst, sb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-          cudaMemcpyAsync(tape_avg(tape, ld, prec, k), s->averages, (size_t)4 * ld * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-          cudaMemcpyAsync(tape_aux(tape, ld, prec, k), s->element_aux, (size_t)2 * ld * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return check_launch("cfd_rk3_step_fixed: tape copy");
-    }
+    launch_stage(&sv, p, MODE_LIMITED, st);
     LimitParams lp;
     memset(&lp, 0, sizeof(lp));
     lp.m = s->mesh;
@@ -1350,14 +1385,11 @@ int cfd_rk3_step_fixed(const CfdSolver* s, const void* q_in, void* q_out, void* 
     lp.stage = stage;
     lp.stage_idx = k;
     lp.gamma = s->gamma;
-    lp.avg = s->averages;
-    lp.aux = s->element_aux;
+    lp.avg = p.avg;
+    lp.aux = p.aux;
     lp.acc = s->acc;
+    lp.pos_out = tape ? tape_pos(tape, ld, prec, k) : nullptr;
     launch_limit(s, lp, st);
-    if (tape && k < 3) {
-      if (cudaMemcpyAsync(tape_state(tape, ld, prec, 2 * k - 1), dst, sb, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return check_launch("cfd_rk3_step_fixed: tape copy");
-    }
   }
   report_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, s->control, s->report, n, s->cfl);
   return check_launch("cfd_rk3_step_fixed");
@@ -1393,6 +1425,7 @@ int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape,
     p.qt = tape_state(tp, ld, prec, 2 * (k - 1));
     p.avg = tape_avg(tp, ld, prec, k);
     p.aux = tape_aux(tp, ld, prec, k);
+    p.pos = tape_pos(tp, ld, prec, k);
     p.qs = k == 1 ? q_in : tape_state(tp, ld, prec, 2 * k - 3);
     p.g = k == 3 ? g_out : (k == 2 ? b2 : b1);
     p.qtb = qtb;

@@ -230,6 +230,19 @@ __device__ __forceinline__ void interface_flux(const R qm[4], const R qp[4], R n
   else hllc(qm, qp, wm, wp, nx, ny, gamma, fm, fp, fhat);
 }
 
+// Interface flux of a face node as the stage kernels use it. The FP32-mixed
+// form returns F(q-).n exactly when the two traces are equal, so a uniform
+// state has no surface term (HLLC's star state would otherwise carry
+// single-precision rounding into every face of a uniform region).
+template <typename R, int FLUX>
+__device__ __forceinline__ void trace_flux(const R qm[4], const R qp[4], R nx, R ny, R gamma, R fhat[4], R fm[4]) {
+  interface_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+  if (sizeof(R) == 4 && qm[0] == qp[0] && qm[1] == qp[1] && qm[2] == qp[2] && qm[3] == qp[3]) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) fhat[c] = fm[c];
+  }
+}
+
 enum { LIM_MINMOD = 0, LIM_MC = 1, LIM_VAN_LEER = 2, LIM_SUPERBEE = 3, LIM_UNLIMITED = 4 };
 
 // limiters.py:16-39

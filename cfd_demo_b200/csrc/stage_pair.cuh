@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_p
     {
       const R* __restrict__ pj = src + e;
       R qn[4];
+      R f0a = R(0), f0b = R(0), g0a = R(0), g0b = R(0);
 #pragma unroll
       for (int c = 0; c < 4; ++c) qn[c] = pj[(c * NP) * ld];
 #pragma unroll
@@ -138,8 +139,19 @@ __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_p
         const R fb = half ? ep * w.u : q[1] * w.u + w.p;
         const R ga = half ? q[2] * w.v + w.p : q[2];
         const R gb = half ? ep * w.v : q[1] * w.v;
-        const R fta = rx * fa + ry * ga, ftb = rx * fb + ry * gb;
-        const R gta = sx * fa + sy * ga, gtb = sx * fb + sy * gb;
+        R fta = rx * fa + ry * ga, ftb = rx * fb + ry * gb;
+        R gta = sx * fa + sy * ga, gtb = sx * fb + sy * gb;
+        if (sizeof(R) == 4) {
+          // FP32 form: differentiate F~ - F~(node 0) ([Dr|Ds] annihilate constants),
+          // so that a uniform state's volume term is exactly zero; with the
+          // rounded tables and metric it would leave a source of one sign in every
+          // element of a uniform region, and mass and energy would drift
+          if (j == 0) {
+            f0a = fta, f0b = ftb, g0a = gta, g0b = gtb;
+            continue;
+          }
+          fta -= f0a, ftb -= f0b, gta -= g0a, gtb -= g0b;
+        }
 #pragma unroll
         for (int i = 0; i < NP; ++i) {
           if (keep_entry<R>(tab::DR[i][j])) {
@@ -207,7 +219,7 @@ __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_p
           const R v = src[idx] + rdt * acc[i][cc];
           if (P.stage_idx == 1) acc[i][cc] = v;
           else if (P.stage_idx == 2) acc[i][cc] = R(0.75) * base[idx] + R(0.25) * v;
-          else acc[i][cc] = base[idx] * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
+          else acc[i][cc] = stage3_combine(base[idx], v);
         }
 #include "stage_epilogue.inc"
     }

@@ -28,6 +28,7 @@ __device__ __forceinline__ void cp_async_small(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // Shared-memory layout of one block (all offsets in elements of R, 16-byte aligned).
 template <typename R, int EPB, bool STAGE_BASE>
@@ -43,9 +44,11 @@ struct TileLayout {
   static constexpr int BYTES = INT_BYTES_OFF + 4 * EPB * 4;
 };
 
-template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE>
-__global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * EPB))
-    stage_tile_kernel(const StageParams P) {
+// MINB: resident blocks per SM the register allocation must allow (the
+// default shapes: 512 / 384 threads per SM for FP32 / FP64; the autotuner
+// also tries a denser one, trading registers for occupancy)
+template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB>
+__global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StageParams P) {
   constexpr int BS = 2 * EPB;
   using L = TileLayout<R, EPB, STAGE_BASE>;
   constexpr int S = L::S;
@@ -119,8 +122,24 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
         cp_async16(&t_int[row * EPB + col], g + e0 + col);
       }
       cp_async_commit();
+      if (!STAGE_BASE && MODE != MODE_RHS && P.stage_idx >= 2) {
+        // the stage base rows are read in the combine, long after this point:
+        // bring the block's rows into L2 now (one 128-byte line per request)
+        constexpr int LPR = (EPB * (int)sizeof(R) + 127) / 128;  // lines per row
+        for (int i = tid; i < 60 * LPR; i += BS) {
+          const int row = i / LPR, ln = i - row * LPR;
+          prefetch_l2(reinterpret_cast<const char*>(base + (size_t)row * ld + e0) + 128 * ln);
+        }
+      }
       cp_async_wait<0>();
       __syncthreads();
+      if (MODE == MODE_LIMITED && P.tape_src) {  // adjoint tape: the stage input, coalesced
+        R* __restrict__ ts = (R*)P.tape_src;
+        for (int i = tid; i < 60 * EPB; i += BS) {
+          const int row = i / EPB, col = i - row * EPB;
+          if (e0 + col < K) ts[(size_t)row * ld + e0 + col] = t_own[row * S + col];
+        }
+      }
     }
     // ---- group B: neighbour face traces (this lane's two variables) and the base rows
     const int finfo = t_int[slot];
@@ -160,6 +179,7 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
     for (int i = 0; i < NP; ++i) acc[i][0] = acc[i][1] = R(0);
 
     // ---- volume term from the own tile (dg.py:148-151)
+    R f0a = R(0), f0b = R(0), g0a = R(0), g0b = R(0);
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
       R q[4];
@@ -171,8 +191,19 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
       const R fb = half ? ep * w.u : q[1] * w.u + w.p;
       const R ga = half ? q[2] * w.v + w.p : q[2];
       const R gb = half ? ep * w.v : q[1] * w.v;
-      const R fta = rx * fa + ry * ga, ftb = rx * fb + ry * gb;
-      const R gta = sx * fa + sy * ga, gtb = sx * fb + sy * gb;
+      R fta = rx * fa + ry * ga, ftb = rx * fb + ry * gb;
+      R gta = sx * fa + sy * ga, gtb = sx * fb + sy * gb;
+      if (sizeof(R) == 4) {
+        // FP32 form: differentiate F~ - F~(node 0) ([Dr|Ds] annihilate constants),
+        // so that a uniform state's volume term is exactly zero; with the
+        // rounded tables and metric it would leave a source of one sign in every
+        // element of a uniform region, and mass and energy would drift
+        if (j == 0) {
+          f0a = fta, f0b = ftb, g0a = gta, g0b = gtb;
+          continue;
+        }
+        fta -= f0a, ftb -= f0b, gta -= g0a, gtb -= g0b;
+      }
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
         if (keep_entry<R>(tab::DR[i][j])) {
@@ -220,7 +251,7 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
           for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
         }
         R fhat[4], fm[4];
-        interface_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+        trace_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
 #pragma unroll
         for (int c = 0; c < 4; ++c) jump[c] = fs * (fm[c] - fhat[c]);
         if (kind != CFD_FACE_INTERIOR) {
@@ -268,7 +299,7 @@ __global__ void __launch_bounds__(2 * EPB, (sizeof(R) == 4 ? 512 : 384) / (2 * E
           const R b = !has_base ? R(0) : (STAGE_BASE ? t_base[row * S + slot] : base[(size_t)row * ld + e]);
           if (P.stage_idx == 1) acc[i][cc] = v;
           else if (P.stage_idx == 2) acc[i][cc] = R(0.75) * b + R(0.25) * v;
-          else acc[i][cc] = b * (R)(1.0 / 3.0) + (R)(2.0 / 3.0) * v;
+          else acc[i][cc] = stage3_combine(b, v);
         }
 #include "stage_epilogue.inc"
     }

@@ -94,27 +94,48 @@ def neighbor_coefficients(connectivity: MeshConnectivity, geometry) -> tuple[np.
     return alpha, beta, partner
 
 
-def check_face_pairing(mesh: TriangleMesh, connectivity: MeshConnectivity, reference, relative_tolerance=1e-9) -> None:
+def check_face_pairing(mesh: TriangleMesh, connectivity: MeshConnectivity, reference, relative_tolerance=1e-9,
+                       *, geometry=None, device=None) -> None:
     """Check by coordinates that face node k of face f meets node 4-k (or k)
     of the neighbour's face, the rule the kernels use (mesh.py:254-291 pairs
-    the nodes by coordinates)."""
-    x, y = node_coordinates(mesh, reference.r, reference.s)
-    fn = reference.face_nodes
+    the nodes by coordinates). With a CUDA ``device`` the check runs there
+    (it dominates the host setup of large meshes)."""
+    geometry = geometry if geometry is not None else element_geometry(mesh)
+    fn = np.asarray(reference.face_nodes)
     nfp = fn.shape[1]
-    lengths = element_geometry(mesh).edge_length
-    for f in range(3):
-        el = np.flatnonzero(connectivity.neighbor_element[:, f] >= 0)
-        if el.size == 0:
-            continue
-        nb = connectivity.neighbor_element[el, f]
-        nf = connectivity.neighbor_face[el, f]
-        same = (f == 2) != (nf == 2)
-        for k in range(nfp):
-            kk = np.where(same, k, nfp - 1 - k)
-            pn = fn[nf, kk]
-            dist = np.hypot(x[fn[f, k], el] - x[pn, nb], y[fn[f, k], el] - y[pn, nb])
-            if np.any(dist > relative_tolerance * lengths[el, f]):
-                raise ValueError("Neighboring face nodes do not coincide; the mesh is not conforming.")
+    r, s = reference.r[fn], reference.s[fn]  # (3, Nfp)
+    bary = np.stack([-(r + s) / 2, (1 + r) / 2, (1 + s) / 2], axis=-1)  # (3, Nfp, 3)
+    nbr, nface = connectivity.neighbor_element, connectivity.neighbor_face
+    k = np.arange(nfp)
+    if device is not None and str(device).startswith("cuda"):
+        import torch
+
+        dev = torch.device(device)
+        corners = torch.as_tensor(mesh.vertices[mesh.elements], device=dev)  # (K, 3, 2)
+        own = torch.einsum("fkv,evd->efkd", torch.as_tensor(bary, device=dev), corners)  # (K, 3, Nfp, 2)
+        nb_t = torch.as_tensor(nbr, device=dev)
+        nf_t = torch.as_tensor(nface, device=dev)
+        e_idx, f_idx = torch.nonzero(nb_t >= 0, as_tuple=True)
+        nb_i, nf_i = nb_t[e_idx, f_idx], nf_t[e_idx, f_idx]
+        same = (f_idx == 2) != (nf_i == 2)
+        kt = torch.arange(nfp, device=dev)
+        kk = torch.where(same[:, None], kt[None, :], nfp - 1 - kt[None, :])  # (M, Nfp)
+        partner = own[nb_i[:, None], nf_i[:, None], kk]  # (M, Nfp, 2)
+        dist = torch.linalg.vector_norm(own[e_idx, f_idx] - partner, dim=-1)
+        tol = relative_tolerance * torch.as_tensor(geometry.edge_length, device=dev)[e_idx, f_idx]
+        bad = bool((dist > tol[:, None]).any())
+    else:
+        corners = mesh.vertices[mesh.elements]
+        own = np.einsum("fkv,evd->efkd", bary, corners)
+        e_idx, f_idx = np.nonzero(nbr >= 0)
+        nb_i, nf_i = nbr[e_idx, f_idx], nface[e_idx, f_idx]
+        same = (f_idx == 2) != (nf_i == 2)
+        kk = np.where(same[:, None], k[None, :], nfp - 1 - k[None, :])
+        partner = own[nb_i[:, None], nf_i[:, None], kk]
+        dist = np.hypot(*np.moveaxis(own[e_idx, f_idx] - partner, -1, 0))
+        bad = bool(np.any(dist > relative_tolerance * geometry.edge_length[e_idx, f_idx][:, None]))
+    if bad:
+        raise ValueError("Neighboring face nodes do not coincide; the mesh is not conforming.")
 
 
 class LimiterOperators(NamedTuple):
@@ -171,9 +192,9 @@ class HostTables:
 
 
 def host_tables(mesh: TriangleMesh, connectivity: MeshConnectivity, geometry, reference, kind: np.ndarray,
-                state: np.ndarray, degree: int = 4) -> HostTables:
+                state: np.ndarray, degree: int = 4, device=None) -> HostTables:
     k = mesh.num_elements
-    check_face_pairing(mesh, connectivity, reference)
+    check_face_pairing(mesh, connectivity, reference, geometry=geometry, device=device)
     alpha, beta, partner = neighbor_coefficients(connectivity, geometry)
     # fixed-state rows: one per distinct exterior state
     fixed = kind == FIXED_STATE

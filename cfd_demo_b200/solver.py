@@ -138,7 +138,7 @@ class EulerSolver:
         self.connectivity = build_connectivity(mesh)
         self.geometry = element_geometry(mesh)
         kind, state = resolve_boundary_conditions(self.connectivity, self.boundary_conditions)
-        self._host = host_tables(mesh, self.connectivity, self.geometry, self.reference, kind, state)
+        self._host = host_tables(mesh, self.connectivity, self.geometry, self.reference, kind, state, device=device)
         self._finish_init(device, block_size, graph_chunk, variant)
 
     def _finish_init(self, device, block_size: int, graph_chunk: int, variant: int = 0) -> None:

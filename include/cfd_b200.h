@@ -166,7 +166,8 @@ typedef struct CfdSolver {
     CfdControl* control;   /* [num_instances] */
     int32_t block_size;    /* threads per block of the pair stage kernel (64, 128, 256); 0 = default */
     int32_t variant;       /* stage kernel: 0 tiled (default), 1 tiled + staged base rows,
-                              2 register-only pair kernel, 3 tiled with 64 elements per block */
+                              2 register-only pair kernel, 3 tiled with 64 elements per block,
+                              4 tiled with registers capped for more resident blocks */
 } CfdSolver;
 
 /* ---- library ------------------------------------------------------------- */
@@ -267,7 +268,10 @@ int cfd_rk3_step_noalloc(const CfdMesh* mesh, int32_t flux, int32_t limiter, int
  * from q_in to q_out without CFL control or rejection; `stage` is scratch of
  * one state. The step report is left in s->report. When `tape` is not NULL it
  * receives what the adjoint needs (cfd_tape_bytes(ld, precision) bytes): the
- * stage states before and after limiting and the stage averages and minima.
+ * stage states before and after limiting, the stage averages and minima, and
+ * the positivity limiter's pressure-scaling theta; the stage kernels write it
+ * as they go (the averages and minima go to the tape instead of
+ * s->averages / s->element_aux).
  * The limiter of every configuration runs in its own kernel here, so the
  * result can differ in the last bits from cfd_rk3_attempt's fused positivity
  * for `unlimited`.

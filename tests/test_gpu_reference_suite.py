@@ -420,3 +420,24 @@ def test_limiter_closed_forms():
     assert np.allclose(mc(r), [0.0, 0.0, 0.5, 0.75, 1.0, 1.5, 2.0])
     assert np.allclose(van_leer(r), [0.0, 0.0, 0.4, 2 / 3, 1.0, 4 / 3, 1.6])
     assert np.allclose(superbee(r), [0.0, 0.0, 0.5, 1.0, 1.0, 2.0, 2.0])
+
+
+def test_face_pairing_check_on_the_gpu():
+    """The setup's coordinate check of the face-node pairing rule, run on the
+    device (the path EulerSolver takes), accepts a conforming mesh and rejects
+    a wrong neighbour face."""
+    import dataclasses
+
+    from cfd_demo_b200 import mesh as pm
+    from cfd_demo_b200.operators import check_face_pairing
+    from cfd_demo_b200.reference_element import build_reference_triangle
+
+    ref = build_reference_triangle(4)
+    m = pm.jittered_rectangle_mesh(40, 30, 0.2, 5)
+    conn, geo = pm.build_connectivity(m), pm.element_geometry(m)
+    check_face_pairing(m, conn, ref, geometry=geo, device="cuda")
+    nf = conn.neighbor_face.copy()
+    e, f = np.argwhere(conn.neighbor_element >= 0)[7]
+    nf[e, f] = (nf[e, f] + 2) % 3
+    with pytest.raises(ValueError, match="not conforming"):
+        check_face_pairing(m, dataclasses.replace(conn, neighbor_face=nf), ref, geometry=geo, device="cuda")

@@ -233,9 +233,10 @@ def test_adjoint_buffer_sizes():
 
     lib = _native.load()
     ld = 128
-    # tape: five stage states (before / after limiting) + 3 x (4 averages + 2 minima) doubles
-    assert lib.cfd_tape_bytes(ld, _native.CFD_FP64) == 5 * 60 * ld * 8 + 18 * ld * 8
-    assert lib.cfd_tape_bytes(ld, _native.CFD_FP32_MIXED) == 5 * 60 * ld * 4 + 18 * ld * 8
+    # tape: five stage states (before / after limiting) + 3 x (4 averages + 3 minima / wave speed
+    # + 2 positivity theta / node) doubles
+    assert lib.cfd_tape_bytes(ld, _native.CFD_FP64) == 5 * 60 * ld * 8 + 27 * ld * 8
+    assert lib.cfd_tape_bytes(ld, _native.CFD_FP32_MIXED) == 5 * 60 * ld * 4 + 27 * ld * 8
     assert lib.cfd_adjoint_work_bytes(ld, _native.CFD_FP64) == 252 * ld * 8 + 4 * ld + 256
     assert lib.cfd_tape_bytes(0, _native.CFD_FP64) == -1
     assert lib.cfd_adjoint_work_bytes(ld, 9) == -1
@@ -249,3 +250,21 @@ def test_package_has_no_oracle_dependency():
             if f.endswith(".py"):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in text and "from oracle" not in text, f
+
+
+def test_face_pairing_check_rejects_a_wrong_neighbour_face():
+    import dataclasses
+
+    from cfd_demo_b200 import mesh as pm
+    from cfd_demo_b200.operators import check_face_pairing
+    from cfd_demo_b200.reference_element import build_reference_triangle
+
+    ref = build_reference_triangle(4)
+    m = pm.jittered_rectangle_mesh(6, 5, 0.2, 1)
+    conn, geo = pm.build_connectivity(m), pm.element_geometry(m)
+    check_face_pairing(m, conn, ref, geometry=geo)
+    nf = conn.neighbor_face.copy()
+    e, f = np.argwhere(conn.neighbor_element >= 0)[0]
+    nf[e, f] = (nf[e, f] + 1) % 3
+    with pytest.raises(ValueError, match="not conforming"):
+        check_face_pairing(m, dataclasses.replace(conn, neighbor_face=nf), ref, geometry=geo)
