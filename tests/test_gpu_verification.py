@@ -101,10 +101,12 @@ def test_transverse_velocity_stays_small(sod_runs):
 @pytest.mark.parametrize("flux,limiter", [("hllc", "van_leer"), ("roe", "superbee")])
 def test_fp32_mixed_meets_the_same_acceptance_checks(flux, limiter, report):
     """The FP32-mixed form on the fine Sod tube: the same L1 and shock
-    thresholds; mass and energy conserved to single-precision round-off."""
+    thresholds; mass, momentum and energy conserved to single-precision
+    round-off (a few 1e-9 measured; a biased stage weight or a source in
+    uniform regions shows up as 1e-5)."""
     r = _analyse(200, 20, flux=flux, limiter=limiter, precision="fp32_mixed")
     report(f"verification Sod 200x20 {flux}/{limiter} FP32-mixed: density L1 {r['errors']['density']:.3e}, "
            f"shock {r['shock']:.5f}; conservation defect {np.abs(r['defect']).max():.2e}")
     assert r["errors"]["density"] <= MAX_DENSITY_L1
     assert abs(r["shock"] - r["exact_shock"]) <= MAX_SHOCK_ERROR
-    assert np.abs(r["defect"]).max() <= 1e-5
+    assert np.abs(r["defect"]).max() <= 1e-7
