@@ -1,6 +1,6 @@
 """Autotuner of the stage-kernel shape (elements per block, tile staging).
 
-The fused stage kernel comes in five shapes (CfdSolver.variant):
+The fused stage kernel comes in six shapes (CfdSolver.variant):
   0  tiled, 32 elements (64 threads) per block, state and geometry staged in
      shared memory, stage base read from global memory in the epilogue
   1  tiled, 32 elements per block, stage base staged in shared memory too
@@ -8,6 +8,8 @@ The fused stage kernel comes in five shapes (CfdSolver.variant):
   3  tiled, 64 elements (128 threads) per block
   4  tiled, 32 elements per block, registers capped so that 10 (FP32) / 8
      (FP64) blocks fit on an SM instead of 8 / 6
+  5  tiled, 64 elements per block, the FP32 face rounds kept rolled (smaller
+     code, LIFT from the constant bank)
 `autotune(solver, state)` times one RK3 attempt per candidate on the solver's
 own buffers (an attempt from the same state recomputes the same step, so the
 candidates see identical work), keeps the fastest, and remembers the choice per
@@ -21,7 +23,7 @@ import math
 
 from . import _native
 
-CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
+CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
 _cache: dict = {}
 
 

@@ -97,6 +97,7 @@ class BatchedEulerSolver:
         s.report = self._ws.report.data_ptr()
         s.control = self._ws.control.data_ptr()
         s.variant = int(variant)
+        s.limit_list = self._ws.limit_list.data_ptr()
         self._struct = s
         self._graph_chunk = int(graph_chunk)
         self._graphs: dict = {}

@@ -277,15 +277,17 @@ __global__ void __launch_bounds__(128) adj_limit_scan_kernel(const AdjParams P) 
   const CfdMesh& m = P.m;
   const int ld = m.ld;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.num_elements || element_instance(m, e) < 0) return;
-  double a[4], eps, pt;
-  R scaled[3][4];
-  bool troubled, need_pos;
-  adj_limit_decide<R, PHI>(P, e, a, eps, pt, scaled, troubled, need_pos);
-  if (troubled || need_pos) {
-    P.list[atomicAdd(P.count, 1)] = e;
-    return;
+  const bool live = e < m.num_elements && element_instance(m, e) >= 0;
+  bool listed = false;
+  if (live) {
+    double a[4], eps, pt;
+    R scaled[3][4];
+    bool troubled, need_pos;
+    adj_limit_decide<R, PHI>(P, e, a, eps, pt, scaled, troubled, need_pos);
+    listed = troubled || need_pos;
   }
+  warp_list_append(P.list, P.count, listed, e);  // every lane of the warp takes part
+  if (!live || listed) return;
   const R* __restrict__ g = (const R*)P.g;
   R* __restrict__ qtb = (R*)P.qtb;
 #pragma unroll 4

@@ -40,6 +40,9 @@ constexpr double POSITIVITY_FLOOR = 1e-13;    // limiting.py:28
 constexpr int BISECTION_STEPS = 60;           // limiting.py:29
 
 enum { MODE_RHS = 0, MODE_LIMITED = 1, MODE_UNLIMITED = 2 };
+// CfdSolver.limit_list: [LIMIT_LIST_HEADER] counters (index = RK stage, 0 for
+// cfd_limit), then the element list
+constexpr int LIMIT_LIST_HEADER = CFD_LIMIT_LIST_HEADER;
 // bits 0-1 decide admissibility; bit 2 marks a NaN CFL step (time_step -> NaN)
 enum { FLAG_NONFINITE = 1, FLAG_BAD_AVERAGE = 2, FLAG_NAN_DT = 4, FLAG_ADMISSIBILITY = 3 };
 
@@ -95,6 +98,19 @@ struct Red {
     fl = 0;
   }
 };
+
+// Appends e to list[] where flag is set, with one atomic per warp on the
+// shared counter (when a large share of the elements is listed, per-thread
+// atomics on one address serialise). All 32 lanes of the warp must call it.
+__device__ __forceinline__ void warp_list_append(int* list, int* count, bool flag, int e) {
+  const unsigned mask = __ballot_sync(0xffffffffu, flag);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (flag) list[base + __popc(mask & ((1u << lane) - 1u))] = e;
+}
 
 __device__ __forceinline__ void commit_one(const Red& r, CfdStageAcc* a) {
 #pragma unroll
@@ -443,30 +459,20 @@ struct LimitParams {
   CfdStageAcc* acc;       // stage mode
   int32_t* troubled_out;  // cfd_limit mode
   double* pos_out;        // optional [2][ld]: pressure-scaling theta and its critical node
+  int* list;              // two-pass form: elements for the rewrite pass, and
+  int* count;             // their number (zeroed before the scan)
 };
 
 // Cockburn-Shu troubled-cell limiter (limiting.py:136-163) followed by the
-// positivity limiter (limiting.py:166-200), in place on the stage state.
-template <typename R, int PHI, int BS>
-__global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
+// positivity limiter (limiting.py:166-200), in place on the stage state, for
+// element e of instance inst. PART 0: everything in one pass; PART 1 (scan):
+// elements the limiters leave as they are contribute their minima, the others
+// are only marked `listed`; PART 2: the rewrite of a listed element.
+template <typename R, int PHI, int PART>
+__device__ __forceinline__ void limit_body(const LimitParams& P, int e, int par, Red& red, bool& listed) {
   const CfdMesh& m = P.m;
   const int ld = m.ld;
-  const int e = blockIdx.x * BS + threadIdx.x;
-  bool live = e < m.num_elements;
-  int inst = 0;
-  if (live && m.instance) inst = m.instance[e];
-  if (inst < 0) {  // padding between instances
-    live = false;
-    inst = 0;
-  }
-  int par = 0;
-  if (live && P.ctl) {
-    live = P.ctl[inst].status == CFD_RUN_ACTIVE;
-    par = P.ctl[inst].parity;
-  }
-  Red red;
-  red.init();
-  if (live) {
+  {
     R* __restrict__ q;
     if (P.stage_idx == 0) {
       q = (R*)P.q_io;
@@ -547,6 +553,10 @@ __global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
         if (d != d) red.fl |= FLAG_NAN_DT;
       }
     } else {
+      if (PART == 1) {  // the scan pass lists the element for the rewrite pass
+        listed = true;
+        return;
+      }
       R s[NP][4];
 #pragma unroll
       for (int i = 0; i < NP; ++i)
@@ -612,11 +622,89 @@ __global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
         if (d != d) red.fl |= FLAG_NAN_DT;
       }
     }
+    }
+}
+
+template <typename R, int PHI, int BS>
+__global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
+  const CfdMesh& m = P.m;
+  const int e = blockIdx.x * BS + threadIdx.x;
+  bool live = e < m.num_elements;
+  int inst = 0;
+  if (live && m.instance) inst = m.instance[e];
+  if (inst < 0) {  // padding between instances
+    live = false;
+    inst = 0;
   }
+  int par = 0;
+  if (live && P.ctl) {
+    live = P.ctl[inst].status == CFD_RUN_ACTIVE;
+    par = P.ctl[inst].parity;
+  }
+  Red red;
+  red.init();
+  bool listed = false;
+  if (live) limit_body<R, PHI, 0>(P, e, par, red, listed);
   if (P.stage_idx == 0) {
     if (live && red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
   } else {
     block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
+  }
+}
+
+// The same limiter in two passes. The scan runs the detection for every
+// element with few registers, commits the minima (and CFL step) of the
+// elements the limiters leave as they are, and lists the others (troubled,
+// or below the positivity floor: a small minority); the rewrite pass then
+// runs the full reconstruction and positivity scaling on the listed
+// elements only, committing their minima one element at a time. Same
+// arithmetic, same results as limit_kernel.
+template <typename R, int PHI, int BS>
+__global__ void __launch_bounds__(BS) limit_scan_kernel(const LimitParams P) {
+  const CfdMesh& m = P.m;
+  const int e = blockIdx.x * BS + threadIdx.x;
+  bool live = e < m.num_elements;
+  int inst = 0;
+  if (live && m.instance) inst = m.instance[e];
+  if (inst < 0) {
+    live = false;
+    inst = 0;
+  }
+  int par = 0;
+  if (live && P.ctl) {
+    live = P.ctl[inst].status == CFD_RUN_ACTIVE;
+    par = P.ctl[inst].parity;
+  }
+  Red red;
+  red.init();
+  bool listed = false;
+  if (live) limit_body<R, PHI, 1>(P, e, par, red, listed);
+  warp_list_append(P.list, P.count, listed, e);
+  if (listed) red.init();
+  if (P.stage_idx == 0) {
+    if (live && red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
+  } else {
+    block_commit<BS>(red, live && !listed, inst, P.acc, 3, P.stage_idx - 1);
+  }
+}
+
+template <typename R, int PHI>
+__global__ void __launch_bounds__(64) limit_rewrite_kernel(const LimitParams P) {
+  const CfdMesh& m = P.m;
+  const int n = *P.count;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int e = P.list[t];
+    const int inst = m.instance ? m.instance[e] : 0;
+    const int par = P.ctl ? P.ctl[inst].parity : 0;
+    Red red;
+    red.init();
+    bool listed = false;
+    limit_body<R, PHI, 2>(P, e, par, red, listed);
+    if (P.stage_idx == 0) {
+      if (red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
+    } else {
+      commit_one(red, P.acc + 3 * inst + (P.stage_idx - 1));
+    }
   }
 }
 
@@ -680,8 +768,9 @@ __global__ void __launch_bounds__(BS) dt_kernel(CfdMesh m, const R* __restrict__
   block_commit<BS>(red, live, inst, acc, 3, 2);
 }
 
-__global__ void reset_acc_kernel(CfdStageAcc* acc, int n) {
+__global__ void reset_acc_kernel(CfdStageAcc* acc, int n, int* list_counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 4 && list_counters) list_counters[i] = 0;  // the two-pass limiter's per-stage counters
   if (i >= n) return;
   CfdStageAcc z;
   z.boundary_flux[0] = z.boundary_flux[1] = z.boundary_flux[2] = z.boundary_flux[3] = 0.0;
@@ -922,7 +1011,7 @@ static int validate(const CfdSolver* s) {
   if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
   if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
     return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
-  if (s->variant < 0 || s->variant > 4) return fail(CFD_E_ARG, "variant must be 0..4");
+  if (s->variant < 0 || s->variant > 5) return fail(CFD_E_ARG, "variant must be 0..5");
   if (s->variant != 2 && s->mesh.instance && s->mesh.num_instances > 1 && (s->mesh.flags & 1) == 0)
     return fail(CFD_E_ARG, "tiled stage kernels need instance ranges aligned to 64 elements (CfdMesh.flags bit 0)");
   return CFD_OK;
@@ -945,17 +1034,18 @@ static void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream
   else if (flux == 1) launch_stage_bs<R, 1, MODE>(p, bs, st);
   else launch_stage_bs<R, 2, MODE>(p, bs, st);
 }
-template <typename R, int FLUX, int MODE, int EPB, bool SB, int MINB = (sizeof(R) == 4 ? 512 : 384) / (2 * EPB)>
+template <typename R, int FLUX, int MODE, int EPB, bool SB, int MINB = (sizeof(R) == 4 ? 512 : 384) / (2 * EPB),
+          bool UF = true>
 static void launch_tile(const StageParams& p, cudaStream_t st) {
   using L = TileLayout<R, EPB, SB>;
   static bool configured = false;  // per instantiation: opt in to > 48 KB of dynamic shared memory
   if (!configured) {
-    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          L::BYTES);
     configured = true;
   }
   const unsigned g = blocks_for(p.m.num_elements, EPB);
-  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB><<<g, 2 * EPB, L::BYTES, st>>>(p);
+  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF><<<g, 2 * EPB, L::BYTES, st>>>(p);
 }
 template <typename R, int FLUX, int MODE>
 static void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_t st) {
@@ -963,6 +1053,7 @@ static void launch_stage_variant(const StageParams& p, int variant, int bs, cuda
   else if (variant == 1) launch_tile<R, FLUX, MODE, 32, true>(p, st);
   else if (variant == 3) launch_tile<R, FLUX, MODE, 64, false>(p, st);
   else if (variant == 4) launch_tile<R, FLUX, MODE, 32, false, sizeof(R) == 4 ? 10 : 8>(p, st);
+  else if (variant == 5) launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, false>(p, st);
   else launch_tile<R, FLUX, MODE, 32, false>(p, st);
 }
 template <typename R, int MODE>
@@ -1001,7 +1092,38 @@ static void launch_limit_phi(const LimitParams& p, int lim, int bs, cudaStream_t
     default: launch_limit_bs<R, 4>(p, bs, st); break;
   }
 }
-static void launch_limit(const CfdSolver* s, const LimitParams& p, cudaStream_t st) {
+template <typename R, int PHI>
+static void launch_limit_two_pass(const LimitParams& p, int bs, cudaStream_t st) {
+  const unsigned g = blocks_for(p.m.num_elements, bs);
+  if (bs == 64) limit_scan_kernel<R, PHI, 64><<<g, 64, 0, st>>>(p);
+  else if (bs == 256) limit_scan_kernel<R, PHI, 256><<<g, 256, 0, st>>>(p);
+  else limit_scan_kernel<R, PHI, 128><<<g, 128, 0, st>>>(p);
+  // the list's length is only known on the device: enough threads for a
+  // quarter of the elements in one sweep (blocks beyond the list end exit at
+  // once; a longer list is swept grid-stride)
+  const unsigned full = blocks_for(p.m.num_elements, 64), cap = 32 * 148;
+  limit_rewrite_kernel<R, PHI><<<full < cap ? full : cap, 64, 0, st>>>(p);
+}
+template <typename R>
+static void launch_limit_two_pass_phi(const LimitParams& p, int lim, int bs, cudaStream_t st) {
+  switch (lim) {
+    case 0: launch_limit_two_pass<R, 0>(p, bs, st); break;
+    case 1: launch_limit_two_pass<R, 1>(p, bs, st); break;
+    case 2: launch_limit_two_pass<R, 2>(p, bs, st); break;
+    case 3: launch_limit_two_pass<R, 3>(p, bs, st); break;
+    default: launch_limit_two_pass<R, 4>(p, bs, st); break;
+  }
+}
+// With a limit_list scratch the limiter runs in two passes (scan + rewrite
+// of the listed elements); without one, in one pass.
+static void launch_limit(const CfdSolver* s, LimitParams p, cudaStream_t st) {
+  if (s->limit_list) {
+    p.count = s->limit_list + (p.stage_idx >= 0 && p.stage_idx <= 3 ? p.stage_idx : 0);
+    p.list = s->limit_list + LIMIT_LIST_HEADER;
+    if (s->precision == CFD_FP64) launch_limit_two_pass_phi<double>(p, s->limiter, bs_of(s), st);
+    else launch_limit_two_pass_phi<float>(p, s->limiter, bs_of(s), st);
+    return;
+  }
   if (s->precision == CFD_FP64) launch_limit_phi<double>(p, s->limiter, bs_of(s), st);
   else launch_limit_phi<float>(p, s->limiter, bs_of(s), st);
 }
@@ -1012,7 +1134,7 @@ static void launch_dt(const CfdSolver* s, const void* q, cudaStream_t st) {
 }
 static void reset_acc(const CfdSolver* s, cudaStream_t st) {
   const int n = 3 * s->mesh.num_instances;
-  reset_acc_kernel<<<blocks_for(n, 128), 128, 0, st>>>(s->acc, n);
+  reset_acc_kernel<<<blocks_for(n > 4 ? n : 4, 128), 128, 0, st>>>(s->acc, n, s->limit_list);
 }
 
 extern "C" {
@@ -1077,6 +1199,8 @@ int cfd_limit(const CfdSolver* s, const void* q_in, void* q_out, int32_t* troubl
   if (!q_in || !q_out || !troubled || !s->averages || !s->element_aux) return fail(CFD_E_ARG, "cfd_limit: null pointer");
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(troubled, 0, sizeof(int32_t) * s->mesh.num_instances, st) != cudaSuccess)
+    return check_launch("cfd_limit: memset");
+  if (s->limit_list && cudaMemsetAsync(s->limit_list, 0, sizeof(int32_t), st) != cudaSuccess)
     return check_launch("cfd_limit: memset");
   const int bs = 128;
   const unsigned g = blocks_for(s->mesh.num_elements, bs);

@@ -46,8 +46,11 @@ struct TileLayout {
 
 // MINB: resident blocks per SM the register allocation must allow (the
 // default shapes: 512 / 384 threads per SM for FP32 / FP64; the autotuner
-// also tries a denser one, trading registers for occupancy)
-template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB>
+// also tries a denser one, trading registers for occupancy). UNROLL_FACES:
+// the FP32 form unrolls the 8 face rounds so the LIFT columns are immediates
+// (more code: 8 inlined flux evaluations); without it the rounds stay rolled
+// and LIFT comes from the constant bank, as in the FP64 form.
+template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB, bool UNROLL_FACES = true>
 __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StageParams P) {
   constexpr int BS = 2 * EPB;
   using L = TileLayout<R, EPB, STAGE_BASE>;
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
     // ---- surface term (dg.py:153-164): 8 rounds, the lanes take nodes 2r and 2r+1;
     // unrolled in the FP32 form so the LIFT columns are compile-time operands
     // (the FP64 form keeps the loop rolled: fewer live registers)
-#pragma unroll(sizeof(R) == 4 ? 8 : 1)
+#pragma unroll((sizeof(R) == 4 && UNROLL_FACES) ? 8 : 1)
     for (int r = 0; r < 8; ++r) {
       const int sl = 2 * r + half;
       R jump[4] = {R(0), R(0), R(0), R(0)};
@@ -267,12 +270,12 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
       const int col = 2 * r;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
-        const R la = sizeof(R) == 4 ? (R)tab::LIFT[i][col] : tabv<R>::lift(i, col);
+        const R la = (sizeof(R) == 4 && UNROLL_FACES) ? (R)tab::LIFT[i][col] : tabv<R>::lift(i, col);
         acc[i][0] = fma(la, ja0, acc[i][0]);
         acc[i][1] = fma(la, ja1, acc[i][1]);
         if (col + 1 < 3 * NFP) {
           const int c1 = col + 1 < 3 * NFP ? col + 1 : col;
-          const R lb = sizeof(R) == 4 ? (R)tab::LIFT[i][c1] : tabv<R>::lift(i, c1);
+          const R lb = (sizeof(R) == 4 && UNROLL_FACES) ? (R)tab::LIFT[i][c1] : tabv<R>::lift(i, c1);
           acc[i][0] = fma(lb, jb0, acc[i][0]);
           acc[i][1] = fma(lb, jb1, acc[i][1]);
         }

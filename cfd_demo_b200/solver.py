@@ -120,6 +120,8 @@ class Workspace:
         self.control = torch.zeros(n * _native.SIZES["CfdControl"], dtype=torch.uint8, device=dev)
         self.small = torch.zeros(max(4 * n, 3 * n, 8), dtype=torch.float64, device=dev)
         self.small_i = torch.zeros(max(n, 8), dtype=torch.int32, device=dev)
+        # the two-pass limiter's counters and element list
+        self.limit_list = torch.zeros(_native.LIMIT_LIST_HEADER + ops.ld, dtype=torch.int32, device=dev)
 
 
 class EulerSolver:
@@ -180,6 +182,7 @@ class EulerSolver:
         s.acc = ws.acc.data_ptr()
         s.report = ws.report.data_ptr()
         s.control = ws.control.data_ptr()
+        s.limit_list = ws.limit_list.data_ptr()
         s.block_size = int(block_size)
         return s
 
@@ -248,7 +251,13 @@ class EulerSolver:
         tmp = torch.empty(self.state_shape, dtype=torch.float64, device=self.operators.device)
         _native.check(self._lib.cfd_unpack_state(x.data_ptr(), tmp.data_ptr(), self.mesh.num_elements,
                                                  self.operators.ld, self.precision, _stream()))
-        return tmp.cpu().numpy()
+        # into page-locked memory (several times the bandwidth of a pageable
+        # copy); the returned array owns its buffer (torch's host cache reuses
+        # the pages once the array is gone)
+        host = torch.empty(self.state_shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(tmp, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return host.numpy()
 
     def _write_control(self, **fields) -> None:
         import torch

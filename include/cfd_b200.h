@@ -64,6 +64,9 @@ extern "C" {
 #define CFD_FACE_SLIP_WALL 1
 #define CFD_FACE_FIXED_STATE 2
 
+/* entries of CfdSolver.limit_list ahead of its element list (counters) */
+#define CFD_LIMIT_LIST_HEADER 16
+
 /* run status (CfdControl.status) */
 #define CFD_RUN_ACTIVE 0
 #define CFD_RUN_DONE 1
@@ -167,7 +170,12 @@ typedef struct CfdSolver {
     int32_t block_size;    /* threads per block of the pair stage kernel (64, 128, 256); 0 = default */
     int32_t variant;       /* stage kernel: 0 tiled (default), 1 tiled + staged base rows,
                               2 register-only pair kernel, 3 tiled with 64 elements per block,
-                              4 tiled with registers capped for more resident blocks */
+                              4 tiled with registers capped for more resident blocks,
+                              5 tiled with 64 elements per block and the face rounds kept rolled */
+    int32_t* limit_list;   /* optional [CFD_LIMIT_LIST_HEADER + ld] scratch: with it the limiter
+                              runs in two passes (a light detection pass over every element,
+                              then the rewrite of the troubled / non-positive ones only);
+                              NULL: one pass. cfd_rk3_begin resets its counters. */
 } CfdSolver;
 
 /* ---- library ------------------------------------------------------------- */

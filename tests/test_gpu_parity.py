@@ -92,7 +92,7 @@ def test_positivity_floor_is_met_exactly():
 
 @pytest.mark.parametrize("flux", FLUXES)
 @pytest.mark.parametrize("limiter", LIMITERS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_step_matches_reference(flux, limiter, variant):
     g = load("step")
     s = make_solver(g, "mesh", flux=flux, limiter=limiter, variant=variant)
@@ -208,7 +208,7 @@ def test_config0_sod_run(report):
     assert np.abs(defect).max() <= 1e-12
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_fp32_mixed_step_tracks_fp64(variant):
     """The FP32-mixed form against the plain form on the step fixture: one RK3
     step agrees to FP32 accuracy (1e-5 of each variable's scale)."""
@@ -220,3 +220,32 @@ def test_fp32_mixed_step_tracks_fp64(variant):
     q32, r32 = s32.step(g["q"], dt)
     assert rel_err(q32, q64) <= 1e-5
     assert r32.admissible and r64.admissible
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
+@pytest.mark.parametrize("limiter", ["minmod", "superbee", "unlimited"])
+def test_two_pass_limiter_is_bitwise_the_one_pass_limiter(limiter, precision):
+    """The limiter's two-pass form (detection scan over every element, then
+    the rewrite of the listed ones) gives the one-pass kernel's results bit
+    for bit: a Sod run (troubled cells and the positivity floor) and one
+    cfd_limit call."""
+    from cfd_demo_b200 import sod_shock_tube
+
+    case = sod_shock_tube(60, 6, flux="hllc", limiter=limiter, precision=precision)
+    s = case.solver
+    assert s.native.limit_list
+    two = s.run(case.initial_state, 0.03)
+    lim_two, count_two = s.limit_with_count(two.state)
+    s.native.limit_list = None
+    s._graphs.clear()
+    one = s.run(case.initial_state, 0.03)
+    lim_one, count_one = s.limit_with_count(two.state)
+    assert np.array_equal(one.state, two.state), np.abs(one.state - two.state).max()
+    assert (one.steps, one.max_troubled_cells, one.rejected_steps) == (two.steps, two.max_troubled_cells,
+                                                                        two.rejected_steps)
+    assert one.min_density == two.min_density and one.min_pressure == two.min_pressure
+    # the boundary-flux integral is a sum of floating-point atomics: its last
+    # bits depend on their order, in either form
+    assert np.allclose(one.boundary_flux_integral, two.boundary_flux_integral, rtol=1e-12, atol=1e-15)
+    assert np.array_equal(lim_one, lim_two), np.abs(lim_one - lim_two).max()
+    assert count_one == count_two
