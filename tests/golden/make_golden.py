@@ -16,7 +16,7 @@ Fixtures (all float64 unless noted):
   limit.npz        apply_limiters for 4 cases x 5 limiters (+ troubled flags)
   step.npz         one SSP-RK3 step for every flux x limiter pair
   sod_short.npz    run() of the 20x2 Sod-like case to t = 0.01
-  sod_config0.npz  run() of the 100x10 Sod tube to t = 0.2 (rusanov/minmod),
+  sod_100x10.npz  run() of the 100x10 Sod tube to t = 0.2 (rusanov/minmod),
                    with per-step dt, report and per-stage troubled counts and
                    the troubled flags of the first 25 steps
 """
@@ -331,14 +331,14 @@ def gen_sod_short(ref):
     return instrumented_run(ref, s, sod_state(ref, s), 0.01, flag_steps=10**6)
 
 
-def gen_sod_config0(ref):
+def gen_sod_100x10(ref):
     case = ref["cases"].sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")
     return instrumented_run(ref, case.solver, case.initial_state, case.final_time, flag_steps=25)
 
 
 GENERATORS = {
     "element": gen_element, "pointwise": gen_pointwise, "rhs": gen_rhs, "limit": gen_limit, "step": gen_step,
-    "sod_short": gen_sod_short, "sod_config0": gen_sod_config0,
+    "sod_short": gen_sod_short, "sod_100x10": gen_sod_100x10,
 }
 
 

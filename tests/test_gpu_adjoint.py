@@ -242,7 +242,7 @@ def test_hold_theta_changes_the_gradient_only_where_positivity_scaled():
     assert not torch.equal(implicit, held)  # the Sod jump drives nodes to the pressure floor
 
 
-def test_config3_sod_400x40_200_steps(report):
+def test_sod_400x40_200_steps_sensitivity(report):
     """The sensitivity study at full size: Sod 400x40 (K = 32,000),
     rusanov/minmod, 200 CFL steps, checkpoints every 20 steps, the bump at its
     seeded position."""

@@ -139,7 +139,7 @@ def test_short_sod_stage_troubled_counts_match_per_step():
         assert rep.admissible
 
 
-def test_config0_sod_trajectory_matches_reference(report):
+def test_sod_100x10_trajectory_matches_reference(report):
     """Sod 100x10 (K=2000), rusanov/minmod, t=0.2, CFL 0.5, marched along the
     reference's own dt sequence (3186 steps). Every step's troubled-cell
     count, stage minima and boundary flux must match the reference's until the
@@ -149,7 +149,7 @@ def test_config0_sod_trajectory_matches_reference(report):
     must agree to 1e-10; after one, its density to 1e-4 in L1."""
     from cfd_demo_b200 import sod_shock_tube
 
-    g = load("sod_config0")
+    g = load("sod_100x10")
     case = sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")
     assert np.array_equal(case.initial_state, g["initial_state"])
     q = case.initial_state
@@ -171,7 +171,7 @@ def test_config0_sod_trajectory_matches_reference(report):
     w = case.solver.reference.cell_weights
     jac = np.asarray(case.solver.geometry.jacobian)
     l1 = float(np.einsum("i,ik,k->", w, np.abs(q[..., 0] - g["state"][..., 0]), jac) / np.einsum("i,k->", w, jac))
-    report(f"config-0 Sod along the reference dt sequence: branch point {branch}, final state rel err {err:.2e}, "
+    report(f"Sod 100x10 along the reference dt sequence: branch point {branch}, final state rel err {err:.2e}, "
            f"L1(rho) {l1:.2e}")
     if branch is None:
         assert err <= 1e-10
@@ -181,7 +181,7 @@ def test_config0_sod_trajectory_matches_reference(report):
         assert l1 <= 1e-4
 
 
-def test_config0_sod_run(report):
+def test_sod_100x10_run_matches_reference(report):
     """The same case through run() with the device CFL dt. The reference
     trajectory holds a troubled-cell decision with a 2e-6 relative margin
     (step 940, element 1870, excess/threshold 0.999998): a 5e-13 state
@@ -190,13 +190,13 @@ def test_config0_sod_run(report):
     and agrees with the reference to round-off up to that step."""
     from cfd_demo_b200 import sod_shock_tube
 
-    g = load("sod_config0")
+    g = load("sod_100x10")
     case = sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")
     res = case.solver.run(case.initial_state, case.final_time)
     w = case.solver.reference.cell_weights
     jac = np.asarray(case.solver.geometry.jacobian)
     l1 = float(np.einsum("i,ik,k->", w, np.abs(res.state[..., 0] - g["state"][..., 0]), jac) / np.einsum("i,k->", w, jac))
-    report(f"config-0 Sod run(): steps {res.steps} (ref {int(g['steps'])}), max troubled {res.max_troubled_cells} "
+    report(f"Sod 100x10 run(): steps {res.steps} (ref {int(g['steps'])}), max troubled {res.max_troubled_cells} "
            f"(ref {int(g['max_troubled_cells'])}), L1(rho) vs ref {l1:.2e}, wall {res.wall_time:.2f} s")
     assert res.steps == int(g["steps"]) and res.rejected_steps == 0
     assert res.time == pytest.approx(0.2, abs=1e-15)
