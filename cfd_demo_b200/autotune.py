@@ -1,6 +1,6 @@
 """Autotuner of the stage-kernel shape (elements per block, tile staging).
 
-The fused stage kernel comes in six shapes (CfdSolver.variant):
+The fused stage kernel comes in nine shapes (CfdSolver.variant):
   0  tiled, 32 elements (64 threads) per block, state and geometry staged in
      shared memory, stage base read from global memory in the epilogue
   1  tiled, 32 elements per block, stage base staged in shared memory too
@@ -10,6 +10,13 @@ The fused stage kernel comes in six shapes (CfdSolver.variant):
      (FP64) blocks fit on an SM instead of 8 / 6
   5  tiled, 64 elements per block, the FP32 face rounds kept rolled (smaller
      code, LIFT from the constant bank)
+  6, 7  variants 3 and 5 with scalar FMAs in the FP32 [Dr|Ds] and LIFT
+     contractions, which every other tiled shape issues as packed FP32x2 FMAs
+     (bitwise the same results; kept as the reference of that claim, not a
+     candidate)
+  8  tiled, 64 elements per block, stage base staged in shared memory (FP32:
+     four blocks still fit an SM's shared memory, as many as the registers
+     allow)
 `autotune(solver, state)` times one RK3 attempt per candidate on the solver's
 own buffers (an attempt from the same state recomputes the same step, so the
 candidates see identical work), keeps the fastest, and remembers the choice per
@@ -23,7 +30,7 @@ import math
 
 from . import _native
 
-CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
+CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (8, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
 _cache: dict = {}
 
 

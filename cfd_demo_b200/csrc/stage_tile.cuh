@@ -38,19 +38,42 @@ struct TileLayout {
   static constexpr int S = sizeof(R) == 4 ? EPB + 8 : EPB + 4;
   static constexpr int OWN = 0;
   static constexpr int BASE = OWN + 60 * S;
-  static constexpr int NBR = BASE + (STAGE_BASE ? 60 * S : 0);  // [8 rounds][4 vars][EPB][2 lanes]
+  // base rows unpadded; the odd lane's rows (30..59) sit 16 words further on,
+  // so the two lanes of a warp still read different banks (saves the padding:
+  // four 64-element FP32 blocks with base rows fit an SM's shared memory)
+  static __device__ __forceinline__ int base_at(int row, int col) { return row * EPB + (row >= 30 ? 16 : 0) + col; }
+  static constexpr int NBR = BASE + (STAGE_BASE ? 60 * EPB + 16 : 0);  // [8 rounds][4 vars][EPB][2 lanes]
   static constexpr int GEO = NBR + 64 * EPB;                      // [13][S]: rx ry sx sy, (nx ny fs) x 3
   static constexpr int INT_BYTES_OFF = (GEO + 13 * S) * (int)sizeof(R);  // int rows [4][EPB]
   static constexpr int BYTES = INT_BYTES_OFF + 4 * EPB * 4;
 };
+
+// y0 += a x0, y1 += a x1. With PACK in the FP32 form: one packed
+// fma.rn.f32x2 (sm_100), each lane rounded exactly like a scalar fmaf, so the
+// results are bitwise those of the two scalar FMAs in one issue slot.
+template <typename R, bool PACK>
+__device__ __forceinline__ void fma_pair(R a, R x0, R x1, R& y0, R& y1) {
+  if constexpr (PACK && sizeof(R) == 4) {
+    const float2 r = __ffma2_rn(make_float2(a, a), make_float2(x0, x1), make_float2(y0, y1));
+    y0 = r.x;
+    y1 = r.y;
+  } else {
+    y0 = fma(a, x0, y0);
+    y1 = fma(a, x1, y1);
+  }
+}
 
 // MINB: resident blocks per SM the register allocation must allow (the
 // default shapes: 512 / 384 threads per SM for FP32 / FP64; the autotuner
 // also tries a denser one, trading registers for occupancy). UNROLL_FACES:
 // the FP32 form unrolls the 8 face rounds so the LIFT columns are immediates
 // (more code: 8 inlined flux evaluations); without it the rounds stay rolled
-// and LIFT comes from the constant bank, as in the FP64 form.
-template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB, bool UNROLL_FACES = true>
+// and LIFT comes from the constant bank, as in the FP64 form. PACK: the
+// [Dr|Ds] and LIFT contractions of the FP32 form as packed FP32x2 FMAs over
+// the lane's two variables (no effect in FP64); every launched FP32 shape
+// packs except the scalar reference shapes.
+template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB, bool UNROLL_FACES = true,
+          bool PACK = false>
 __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StageParams P) {
   constexpr int BS = 2 * EPB;
   using L = TileLayout<R, EPB, STAGE_BASE>;
@@ -168,7 +191,7 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
       constexpr int CPR = EPB / VEC;
       for (int ch = tid; ch < 60 * CPR; ch += BS) {
         const int row = ch / CPR, col = (ch - row * CPR) * VEC;
-        cp_async16(&t_base[row * S + col], base + (size_t)row * ld + e0 + col);
+        cp_async16(&t_base[L::base_at(row, col)], base + (size_t)row * ld + e0 + col);
       }
     }
     cp_async_commit();
@@ -209,14 +232,8 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
       }
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
-        if (keep_entry<R>(tab::DR[i][j])) {
-          acc[i][0] = fma((R)(-tab::DR[i][j]), fta, acc[i][0]);
-          acc[i][1] = fma((R)(-tab::DR[i][j]), ftb, acc[i][1]);
-        }
-        if (keep_entry<R>(tab::DS[i][j])) {
-          acc[i][0] = fma((R)(-tab::DS[i][j]), gta, acc[i][0]);
-          acc[i][1] = fma((R)(-tab::DS[i][j]), gtb, acc[i][1]);
-        }
+        if (keep_entry<R>(tab::DR[i][j])) fma_pair<R, PACK>((R)(-tab::DR[i][j]), fta, ftb, acc[i][0], acc[i][1]);
+        if (keep_entry<R>(tab::DS[i][j])) fma_pair<R, PACK>((R)(-tab::DS[i][j]), gta, gtb, acc[i][0], acc[i][1]);
       }
     }
 
@@ -271,13 +288,11 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
         const R la = (sizeof(R) == 4 && UNROLL_FACES) ? (R)tab::LIFT[i][col] : tabv<R>::lift(i, col);
-        acc[i][0] = fma(la, ja0, acc[i][0]);
-        acc[i][1] = fma(la, ja1, acc[i][1]);
+        fma_pair<R, PACK>(la, ja0, ja1, acc[i][0], acc[i][1]);
         if (col + 1 < 3 * NFP) {
           const int c1 = col + 1 < 3 * NFP ? col + 1 : col;
           const R lb = (sizeof(R) == 4 && UNROLL_FACES) ? (R)tab::LIFT[i][c1] : tabv<R>::lift(i, c1);
-          acc[i][0] = fma(lb, jb0, acc[i][0]);
-          acc[i][1] = fma(lb, jb1, acc[i][1]);
+          fma_pair<R, PACK>(lb, jb0, jb1, acc[i][0], acc[i][1]);
         }
       }
     }
@@ -299,7 +314,7 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
         for (int cc = 0; cc < 2; ++cc) {
           const int row = (c0 + cc) * NP + i;
           const R v = t_own[row * S + slot] + rdt * acc[i][cc];
-          const R b = !has_base ? R(0) : (STAGE_BASE ? t_base[row * S + slot] : base[(size_t)row * ld + e]);
+          const R b = !has_base ? R(0) : (STAGE_BASE ? t_base[L::base_at(row, slot)] : base[(size_t)row * ld + e]);
           if (P.stage_idx == 1) acc[i][cc] = v;
           else if (P.stage_idx == 2) acc[i][cc] = R(0.75) * b + R(0.25) * v;
           else acc[i][cc] = stage3_combine(b, v);

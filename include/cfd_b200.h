@@ -171,7 +171,11 @@ typedef struct CfdSolver {
     int32_t variant;       /* stage kernel: 0 tiled (default), 1 tiled + staged base rows,
                               2 register-only pair kernel, 3 tiled with 64 elements per block,
                               4 tiled with registers capped for more resident blocks,
-                              5 tiled with 64 elements per block and the face rounds kept rolled */
+                              5 tiled with 64 elements per block and the face rounds kept rolled,
+                              6 / 7 as 3 / 5 with scalar FMAs in the FP32 [Dr|Ds] and LIFT
+                              contractions, which the other tiled shapes issue as packed
+                              FP32x2 FMAs (bitwise the same results; FP64 runs 3 / 5),
+                              8 tiled with 64 elements per block + staged base rows */
     int32_t* limit_list;   /* optional [CFD_LIMIT_LIST_HEADER + ld] scratch: with it the limiter
                               runs in two passes (a light detection pass over every element,
                               then the rewrite of the troubled / non-positive ones only);

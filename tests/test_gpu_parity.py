@@ -92,7 +92,7 @@ def test_positivity_floor_is_met_exactly():
 
 @pytest.mark.parametrize("flux", FLUXES)
 @pytest.mark.parametrize("limiter", LIMITERS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_step_matches_reference(flux, limiter, variant):
     g = load("step")
     s = make_solver(g, "mesh", flux=flux, limiter=limiter, variant=variant)
@@ -208,7 +208,7 @@ def test_sod_100x10_run_matches_reference(report):
     assert np.abs(defect).max() <= 1e-12
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_fp32_mixed_step_tracks_fp64(variant):
     """The FP32-mixed form against the plain form on the step fixture: one RK3
     step agrees to FP32 accuracy (1e-5 of each variable's scale)."""
@@ -249,3 +249,24 @@ def test_two_pass_limiter_is_bitwise_the_one_pass_limiter(limiter, precision):
     assert np.allclose(one.boundary_flux_integral, two.boundary_flux_integral, rtol=1e-12, atol=1e-15)
     assert np.array_equal(lim_one, lim_two), np.abs(lim_one - lim_two).max()
     assert count_one == count_two
+
+
+@pytest.mark.parametrize("flux", FLUXES)
+@pytest.mark.parametrize("scalar,packed", [(6, 3), (7, 5)])
+def test_packed_fp32_contractions_are_bitwise_the_scalar_ones(flux, scalar, packed):
+    """The tiled shapes issue the FP32 [Dr|Ds] and LIFT contractions as packed
+    FP32x2 FMAs; variants 6 / 7 are shapes 3 / 5 with scalar FMAs. Each packed
+    lane rounds like a scalar FMA, so a Sod run and one RHS agree bit for bit."""
+    from cfd_demo_b200 import sod_shock_tube
+
+    out = {}
+    for v in (scalar, packed):
+        case = sod_shock_tube(60, 6, flux=flux, limiter="minmod", precision="fp32_mixed")
+        case.solver.set_variant(v)
+        res = case.solver.run(case.initial_state, 0.02)
+        rhs, _ = case.solver.rhs(res.state)
+        out[v] = (res, rhs)
+    (a, ra), (b, rb) = out[scalar], out[packed]
+    assert a.steps == b.steps and a.max_troubled_cells == b.max_troubled_cells
+    assert np.array_equal(a.state, b.state), np.abs(a.state - b.state).max()
+    assert np.array_equal(ra, rb), np.abs(ra - rb).max()
