@@ -63,7 +63,7 @@ FALLBACK_HBM_GBS = 6650.0
 # proportion to K): profiles/stage_tile_fp32_512x512.md and
 # profiles/stage_tile_fp64_512x512.md. Writes still in L2 when a launch ends
 # are not counted there, so the stage result's 240 / 480 B appear partly.
-NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (482.2, 741.1, 748.2), "fp64": (1011.6, 1516.0, 1524.7)}
+NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (481.5, 739.6, 747.7), "fp64": (1007.6, 1515.6, 1521.4)}
 
 
 def stage_bytes(real_bytes: int) -> list[int]:

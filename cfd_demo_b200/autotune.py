@@ -1,6 +1,6 @@
 """Autotuner of the stage-kernel shape (elements per block, tile staging).
 
-The fused stage kernel comes in nine shapes (CfdSolver.variant):
+The fused stage kernel comes in ten shapes (CfdSolver.variant):
   0  tiled, 32 elements (64 threads) per block, state and geometry staged in
      shared memory, stage base read from global memory in the epilogue
   1  tiled, 32 elements per block, stage base staged in shared memory too
@@ -17,6 +17,8 @@ The fused stage kernel comes in nine shapes (CfdSolver.variant):
   8  tiled, 64 elements per block, stage base staged in shared memory (FP32:
      four blocks still fit an SM's shared memory, as many as the registers
      allow)
+  9  shape 8 with the face-node flux as an out-of-line call, so the eight
+     unrolled face rounds share one copy of the flux code (FP32; FP64 runs 8)
 `autotune(solver, state)` times one RK3 attempt per candidate on the solver's
 own buffers (an attempt from the same state recomputes the same step, so the
 candidates see identical work), keeps the fastest, and remembers the choice per
@@ -30,7 +32,7 @@ import math
 
 from . import _native
 
-CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (8, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
+CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (8, 0), (9, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
 _cache: dict = {}
 
 

@@ -1011,7 +1011,7 @@ static int validate(const CfdSolver* s) {
   if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
   if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
     return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
-  if (s->variant < 0 || s->variant > 8) return fail(CFD_E_ARG, "variant must be 0..8");
+  if (s->variant < 0 || s->variant > 9) return fail(CFD_E_ARG, "variant must be 0..9");
   if (s->variant != 2 && s->mesh.instance && s->mesh.num_instances > 1 && (s->mesh.flags & 1) == 0)
     return fail(CFD_E_ARG, "tiled stage kernels need instance ranges aligned to 64 elements (CfdMesh.flags bit 0)");
   return CFD_OK;
@@ -1035,18 +1035,19 @@ static void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream
   else launch_stage_bs<R, 2, MODE>(p, bs, st);
 }
 template <typename R, int FLUX, int MODE, int EPB, bool SB, int MINB = (sizeof(R) == 4 ? 512 : 384) / (2 * EPB),
-          bool UF = true, bool PK = true>
+          bool UF = true, bool PK = true, bool CF = false>
 static void launch_tile(const StageParams& p, cudaStream_t st) {
   using L = TileLayout<R, EPB, SB>;
   constexpr bool PACK = PK && sizeof(R) == 4;  // FP64 shares the unpacked instantiation
+  constexpr bool CALL = CF && sizeof(R) == 4;
   static bool configured = false;  // per instantiation: opt in to > 48 KB of dynamic shared memory
   if (!configured) {
-    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK>,
+    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
     configured = true;
   }
   const unsigned g = blocks_for(p.m.num_elements, EPB);
-  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK><<<g, 2 * EPB, L::BYTES, st>>>(p);
+  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL><<<g, 2 * EPB, L::BYTES, st>>>(p);
 }
 template <typename R, int FLUX, int MODE>
 static void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_t st) {
@@ -1059,6 +1060,7 @@ static void launch_stage_variant(const StageParams& p, int variant, int bs, cuda
   else if (variant == 6) launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, true, false>(p, st);
   else if (variant == 7) launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, false, false>(p, st);
   else if (variant == 8) launch_tile<R, FLUX, MODE, 64, true>(p, st);
+  else if (variant == 9) launch_tile<R, FLUX, MODE, 64, true, (sizeof(R) == 4 ? 512 : 384) / 128, true, true, true>(p, st);
   else launch_tile<R, FLUX, MODE, 32, false>(p, st);
 }
 template <typename R, int MODE>

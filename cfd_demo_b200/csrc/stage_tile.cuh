@@ -63,6 +63,20 @@ __device__ __forceinline__ void fma_pair(R a, R x0, R x1, R& y0, R& y1) {
   }
 }
 
+// The interface flux of one face node as an out-of-line call (CALL_FLUX):
+// the eight unrolled face rounds then share one copy of the flux code, which
+// keeps the kernel's instruction footprint small, while the LIFT columns stay
+// immediates.
+template <typename R> struct NodeFlux { R fhat[4], fm[4]; };
+template <typename R, int FLUX>
+__device__ __noinline__ NodeFlux<R> trace_flux_call(R m0, R m1, R m2, R m3, R p0, R p1, R p2, R p3, R nx, R ny,
+                                                    R gamma) {
+  const R qm[4] = {m0, m1, m2, m3}, qp[4] = {p0, p1, p2, p3};
+  NodeFlux<R> o;
+  trace_flux<R, FLUX>(qm, qp, nx, ny, gamma, o.fhat, o.fm);
+  return o;
+}
+
 // MINB: resident blocks per SM the register allocation must allow (the
 // default shapes: 512 / 384 threads per SM for FP32 / FP64; the autotuner
 // also tries a denser one, trading registers for occupancy). UNROLL_FACES:
@@ -71,9 +85,10 @@ __device__ __forceinline__ void fma_pair(R a, R x0, R x1, R& y0, R& y1) {
 // and LIFT comes from the constant bank, as in the FP64 form. PACK: the
 // [Dr|Ds] and LIFT contractions of the FP32 form as packed FP32x2 FMAs over
 // the lane's two variables (no effect in FP64); every launched FP32 shape
-// packs except the scalar reference shapes.
+// packs except the scalar reference shapes. CALL_FLUX: the face-node flux
+// as a call instead of eight inlined copies (FP32 form).
 template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB, bool UNROLL_FACES = true,
-          bool PACK = false>
+          bool PACK = false, bool CALL_FLUX = false>
 __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StageParams P) {
   constexpr int BS = 2 * EPB;
   using L = TileLayout<R, EPB, STAGE_BASE>;
@@ -271,7 +286,14 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
           for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
         }
         R fhat[4], fm[4];
-        trace_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+        if constexpr (CALL_FLUX) {
+          const NodeFlux<R> o = trace_flux_call<R, FLUX>(qm[0], qm[1], qm[2], qm[3], qp[0], qp[1], qp[2], qp[3], nx,
+                                                         ny, gamma);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) fhat[c] = o.fhat[c], fm[c] = o.fm[c];
+        } else {
+          trace_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
+        }
 #pragma unroll
         for (int c = 0; c < 4; ++c) jump[c] = fs * (fm[c] - fhat[c]);
         if (kind != CFD_FACE_INTERIOR) {

@@ -175,7 +175,8 @@ typedef struct CfdSolver {
                               6 / 7 as 3 / 5 with scalar FMAs in the FP32 [Dr|Ds] and LIFT
                               contractions, which the other tiled shapes issue as packed
                               FP32x2 FMAs (bitwise the same results; FP64 runs 3 / 5),
-                              8 tiled with 64 elements per block + staged base rows */
+                              8 tiled with 64 elements per block + staged base rows,
+                              9 as 8 with the face-node flux as an out-of-line call (FP32) */
     int32_t* limit_list;   /* optional [CFD_LIMIT_LIST_HEADER + ld] scratch: with it the limiter
                               runs in two passes (a light detection pass over every element,
                               then the rewrite of the troubled / non-positive ones only);
