@@ -340,11 +340,12 @@ def run_ours(args, rank: int, world: int) -> dict | None:
 
     tuned = {}
     for name, solver in (("fp32_mixed", fp32), ("fp64", fp64)):
-        if args.variant is None:
+        variant = args.variant_fp64 if name == "fp64" and args.variant_fp64 is not None else args.variant
+        if variant is None:
             tuned[name] = autotune(solver, q0)
         else:
-            solver.set_variant(args.variant)
-            tuned[name] = {"choice": (args.variant, 0), "ms": {}}
+            solver.set_variant(variant)
+            tuned[name] = {"choice": (variant, 0), "ms": {}}
     k = fp32.mesh.num_elements
     dof = k * NP_NODES
 
@@ -581,8 +582,15 @@ def run_precision(args) -> dict:
                          SOD_GAMMA, SOD_DISCONTINUITY)
     t_end = case.final_time
     waves = exact.wave_positions(t_end)
-    out, states = {}, {}
+    from cfd_demo_b200.autotune import autotune
+
+    out, states, shapes = {}, {}, {}
     for name, solver in solvers.items():
+        if args.variant is None:  # stage-kernel shape picked outside the timed run
+            shapes[name] = autotune(solver, case.initial_state)["choice"]
+        else:
+            solver.set_variant(args.variant)
+            shapes[name] = (args.variant, 0)
         initial = solver.integrate(case.initial_state)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -600,7 +608,7 @@ def run_precision(args) -> dict:
             "contact_x": front_position(cols, faces, (waves["contact"] - 0.05, waves["contact"] + 0.05)),
             "mass_defect": float(defect[0]), "energy_defect": float(defect[3]),
             "max_troubled_cells": res.max_troubled_cells, "min_density": res.min_density,
-            "min_pressure": res.min_pressure,
+            "min_pressure": res.min_pressure, "stage_kernel": shapes[name],
         }
     d = (states["fp32_mixed"][..., 0] - states["fp64"][..., 0]).abs()
     w = torch.as_tensor(case.solver.reference.cell_weights, device=d.device, dtype=d.dtype)
@@ -645,6 +653,10 @@ def main() -> None:
     ap.add_argument("--cpu-baseline-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="stage-kernel variant (default: autotuned)")
+    ap.add_argument("--variant-fp64", type=int, default=None,
+                    help="stage-kernel variant of the FP64 form (default: as --variant); fixing both to the "
+                         "autotuner's choices reproduces a run's kernels under a profiler, whose serialised "
+                         "launches would mislead the autotuner")
     ap.add_argument("--workload", choices=["microbenchmark", "batch", "adjoint", "precision"], default="microbenchmark")
     ap.add_argument("--precision-nx", type=int, default=2000)
     ap.add_argument("--precision-quad", type=int, default=6)
