@@ -113,8 +113,8 @@ def check_face_pairing(mesh: TriangleMesh, connectivity: MeshConnectivity, refer
         dev = torch.device(device)
         corners = torch.as_tensor(mesh.vertices[mesh.elements], device=dev)  # (K, 3, 2)
         own = torch.einsum("fkv,evd->efkd", torch.as_tensor(bary, device=dev), corners)  # (K, 3, Nfp, 2)
-        nb_t = torch.as_tensor(nbr, device=dev)
-        nf_t = torch.as_tensor(nface, device=dev)
+        nb_t = torch.as_tensor(np.array(nbr), device=dev)  # copies: the tables are read-only
+        nf_t = torch.as_tensor(np.array(nface), device=dev)
         e_idx, f_idx = torch.nonzero(nb_t >= 0, as_tuple=True)
         nb_i, nf_i = nb_t[e_idx, f_idx], nf_t[e_idx, f_idx]
         same = (f_idx == 2) != (nf_i == 2)
@@ -122,7 +122,7 @@ def check_face_pairing(mesh: TriangleMesh, connectivity: MeshConnectivity, refer
         kk = torch.where(same[:, None], kt[None, :], nfp - 1 - kt[None, :])  # (M, Nfp)
         partner = own[nb_i[:, None], nf_i[:, None], kk]  # (M, Nfp, 2)
         dist = torch.linalg.vector_norm(own[e_idx, f_idx] - partner, dim=-1)
-        tol = relative_tolerance * torch.as_tensor(geometry.edge_length, device=dev)[e_idx, f_idx]
+        tol = relative_tolerance * torch.as_tensor(np.array(geometry.edge_length), device=dev)[e_idx, f_idx]
         bad = bool((dist > tol[:, None]).any())
     else:
         corners = mesh.vertices[mesh.elements]
