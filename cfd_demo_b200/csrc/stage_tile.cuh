@@ -63,6 +63,39 @@ __device__ __forceinline__ void fma_pair(R a, R x0, R x1, R& y0, R& y1) {
   }
 }
 
+// (y0, y1) = a (f0, f1) + b (g0, g1): a contravariant flux pair. The FP32 form
+// fixes the rounding as fma(b, g, a f), one packed FMUL2 + FFMA2 with PACK
+// (bitwise the scalar pair); FP64 keeps the plain expression.
+template <typename R, bool PACK>
+__device__ __forceinline__ void lin_pair(R a, R b, R f0, R f1, R g0, R g1, R& y0, R& y1) {
+  if constexpr (sizeof(R) == 4) {
+    if constexpr (PACK) {
+      const float2 r = __ffma2_rn(make_float2(b, b), make_float2(g0, g1),
+                                  __fmul2_rn(make_float2(a, a), make_float2(f0, f1)));
+      y0 = r.x;
+      y1 = r.y;
+    } else {
+      y0 = fmaf(b, g0, a * f0);
+      y1 = fmaf(b, g1, a * f1);
+    }
+  } else {
+    y0 = a * f0 + b * g0;
+    y1 = a * f1 + b * g1;
+  }
+}
+// (y0, y1) -= (d0, d1), one packed FADD2 of the negated pair with PACK.
+template <typename R, bool PACK>
+__device__ __forceinline__ void sub_pair(R& y0, R& y1, R d0, R d1) {
+  if constexpr (PACK && sizeof(R) == 4) {
+    const float2 r = __fadd2_rn(make_float2(y0, y1), make_float2(-d0, -d1));
+    y0 = r.x;
+    y1 = r.y;
+  } else {
+    y0 -= d0;
+    y1 -= d1;
+  }
+}
+
 // The interface flux of one face node as an out-of-line call (CALL_FLUX):
 // the eight unrolled face rounds then share one copy of the flux code, which
 // keeps the kernel's instruction footprint small, while the LIFT columns stay
@@ -232,8 +265,9 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
       const R fb = half ? ep * w.u : q[1] * w.u + w.p;
       const R ga = half ? q[2] * w.v + w.p : q[2];
       const R gb = half ? ep * w.v : q[1] * w.v;
-      R fta = rx * fa + ry * ga, ftb = rx * fb + ry * gb;
-      R gta = sx * fa + sy * ga, gtb = sx * fb + sy * gb;
+      R fta, ftb, gta, gtb;
+      lin_pair<R, PACK>(rx, ry, fa, fb, ga, gb, fta, ftb);
+      lin_pair<R, PACK>(sx, sy, fa, fb, ga, gb, gta, gtb);
       if (sizeof(R) == 4) {
         // FP32 form: differentiate F~ - F~(node 0) ([Dr|Ds] annihilate constants),
         // so that a uniform state's volume term is exactly zero; with the
@@ -243,7 +277,8 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
           f0a = fta, f0b = ftb, g0a = gta, g0b = gtb;
           continue;
         }
-        fta -= f0a, ftb -= f0b, gta -= g0a, gtb -= g0b;
+        sub_pair<R, PACK>(fta, ftb, f0a, f0b);
+        sub_pair<R, PACK>(gta, gtb, g0a, g0b);
       }
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
