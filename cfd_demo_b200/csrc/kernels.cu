@@ -1040,11 +1040,17 @@ static void launch_tile(const StageParams& p, cudaStream_t st) {
   using L = TileLayout<R, EPB, SB>;
   constexpr bool PACK = PK && sizeof(R) == 4;  // FP64 shares the unpacked instantiation
   constexpr bool CALL = CF && sizeof(R) == 4;
-  static bool configured = false;  // per instantiation: opt in to > 48 KB of dynamic shared memory
-  if (!configured) {
+  // opt in to > 48 KB of dynamic shared memory, once per instantiation and
+  // device (the attribute belongs to the device's context); setting it twice
+  // is harmless, so concurrent first calls need no lock
+  constexpr int MAX_DEV = 64;
+  static bool configured[MAX_DEV] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= MAX_DEV || !configured[dev]) {
     cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
-    configured = true;
+    if (dev >= 0 && dev < MAX_DEV) configured[dev] = true;
   }
   const unsigned g = blocks_for(p.m.num_elements, EPB);
   stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL><<<g, 2 * EPB, L::BYTES, st>>>(p);
