@@ -96,6 +96,50 @@ __device__ __forceinline__ void sub_pair(R& y0, R& y1, R d0, R d1) {
   }
 }
 
+// SSP-RK3 stage combine of a lane's pair of values: v = own + dt acc, then
+// stage 1: v; stage 2: 3/4 b + 1/4 v; stage 3: b + 2/3 (v - b). The FP32 form
+// fixes the roundings (fma(dt, acc, own), fma(1/4, v, 3/4 b), fma(2/3, v - b,
+// b)), as packed FP32x2 operations with PACK (bitwise the scalar pair); FP64
+// keeps the reference's expressions.
+template <typename R, bool PACK>
+__device__ __forceinline__ void combine_pair(int stage, R rdt, R o0, R o1, R b0, R b1, R& a0, R& a1) {
+  if constexpr (sizeof(R) == 4) {
+    if constexpr (PACK) {
+      const float2 v = __ffma2_rn(make_float2(rdt, rdt), make_float2(a0, a1), make_float2(o0, o1));
+      float2 r = v;
+      if (stage == 2)
+        r = __ffma2_rn(make_float2(0.25f, 0.25f), v, __fmul2_rn(make_float2(0.75f, 0.75f), make_float2(b0, b1)));
+      else if (stage == 3)
+        r = __ffma2_rn(make_float2(2.0f / 3.0f, 2.0f / 3.0f), __fadd2_rn(v, make_float2(-b0, -b1)),
+                       make_float2(b0, b1));
+      a0 = r.x;
+      a1 = r.y;
+    } else {
+      const float v0 = fmaf(rdt, a0, o0), v1 = fmaf(rdt, a1, o1);
+      if (stage == 1) a0 = v0, a1 = v1;
+      else if (stage == 2) a0 = fmaf(0.25f, v0, 0.75f * b0), a1 = fmaf(0.25f, v1, 0.75f * b1);
+      else a0 = fmaf(2.0f / 3.0f, v0 - b0, b0), a1 = fmaf(2.0f / 3.0f, v1 - b1, b1);
+    }
+  } else {
+    const R v0 = o0 + rdt * a0, v1 = o1 + rdt * a1;
+    if (stage == 1) a0 = v0, a1 = v1;
+    else if (stage == 2) a0 = R(0.75) * b0 + R(0.25) * v0, a1 = R(0.75) * b1 + R(0.25) * v1;
+    else a0 = stage3_combine(b0, v0), a1 = stage3_combine(b1, v1);
+  }
+}
+// (j0, j1) = s ((m0, m1) - (h0, h1)), packed with PACK (bitwise the scalar pair).
+template <typename R, bool PACK>
+__device__ __forceinline__ void jump_pair(R s, R m0, R m1, R h0, R h1, R& j0, R& j1) {
+  if constexpr (PACK && sizeof(R) == 4) {
+    const float2 r = __fmul2_rn(make_float2(s, s), __fadd2_rn(make_float2(m0, m1), make_float2(-h0, -h1)));
+    j0 = r.x;
+    j1 = r.y;
+  } else {
+    j0 = s * (m0 - h0);
+    j1 = s * (m1 - h1);
+  }
+}
+
 // The interface flux of one face node as an out-of-line call (CALL_FLUX):
 // the eight unrolled face rounds then share one copy of the flux code, which
 // keeps the kernel's instruction footprint small, while the LIFT columns stay
@@ -329,8 +373,8 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
         } else {
           trace_flux<R, FLUX>(qm, qp, nx, ny, gamma, fhat, fm);
         }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) jump[c] = fs * (fm[c] - fhat[c]);
+        jump_pair<R, PACK>(fs, fm[0], fm[1], fhat[0], fhat[1], jump[0], jump[1]);
+        jump_pair<R, PACK>(fs, fm[2], fm[3], fhat[2], fhat[3], jump[2], jump[3]);
         if (kind != CFD_FACE_INTERIOR) {
           const double bw = ctab::FACE_W[k] * m.face_hlen[(size_t)f * ld + e];
 #pragma unroll
@@ -366,16 +410,16 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
       // ---- SSP-RK3 stage combine (time_integration.py:61-66)
       const R rdt = (R)dt;
 #pragma unroll
-      for (int i = 0; i < NP; ++i)
+      for (int i = 0; i < NP; ++i) {
+        R o[2], b[2];
 #pragma unroll
         for (int cc = 0; cc < 2; ++cc) {
           const int row = (c0 + cc) * NP + i;
-          const R v = t_own[row * S + slot] + rdt * acc[i][cc];
-          const R b = !has_base ? R(0) : (STAGE_BASE ? t_base[L::base_at(row, slot)] : base[(size_t)row * ld + e]);
-          if (P.stage_idx == 1) acc[i][cc] = v;
-          else if (P.stage_idx == 2) acc[i][cc] = R(0.75) * b + R(0.25) * v;
-          else acc[i][cc] = stage3_combine(b, v);
+          o[cc] = t_own[row * S + slot];
+          b[cc] = !has_base ? R(0) : (STAGE_BASE ? t_base[L::base_at(row, slot)] : base[(size_t)row * ld + e]);
         }
+        combine_pair<R, PACK>(P.stage_idx, rdt, o[0], o[1], b[0], b[1], acc[i][0], acc[i][1]);
+      }
 #include "stage_epilogue.inc"
     }
   }
