@@ -45,10 +45,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "DOF-steps/s FP32-mixed vs FP64 plain at L1(rho)<=1e-5; adjoint/forward time"
-NX = 724
-JITTER = 0.2
-MESH_SEED = 20261203
-FIELD_SEED = 7
+from cfd_demo_b200.workloads import JITTER, NX  # noqa: E402
+
 NP_NODES = 15
 FALLBACK_HBM_GBS = 6650.0
 # Algorithmic bytes per element per RK3 step of the three stage launches:
@@ -60,9 +58,8 @@ FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_write.sum) measured by ncu on the tiled stage kernel at 512x512
 # quads (K = 524,288; the 724x724 workload is too large for a full capture),
 # scaled to a launch of the benchmark by its element count (traffic grows in
-# proportion to K): profiles/stage_tile_fp32_512x512.md and
-# profiles/stage_tile_fp64_512x512.md. Writes still in L2 when a launch ends
-# are not counted there, so the stage result's 240 / 480 B appear partly.
+# proportion to K). Writes still in L2 when a launch ends are not counted
+# there, so the stage result's 240 / 480 B appear partly.
 NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (481.5, 739.6, 747.7), "fp64": (1007.6, 1515.6, 1521.4)}
 
 
@@ -73,45 +70,11 @@ def stage_bytes(real_bytes: int) -> list[int]:
 
 
 # ---------------------------------------------------------------- workload ---
-def fourier_field(x, y, rng, lo, hi, xp):
-    """Sum of 8 random Fourier modes, mapped affinely onto [lo, hi]."""
-    f = xp.zeros_like(x)
-    for _ in range(8):
-        kx, ky = rng.integers(1, 5, size=2)
-        amp = rng.uniform(0.3, 1.0)
-        ph = rng.uniform(0.0, 2 * math.pi)
-        f = f + amp * xp.cos(2 * math.pi * (float(kx) * x + float(ky) * y) + ph)
-    fmin, fmax = f.min(), f.max()
-    return lo + (hi - lo) * (f - fmin) / (fmax - fmin)
-
-
 def make_workload(nx: int = NX, precision: str = "fp32_mixed", device="cuda"):
     """(solver, initial state as a device (Np, K, 4) float64 tensor)."""
-    import torch
+    from cfd_demo_b200.workloads import microbenchmark
 
-    from cfd_demo_b200 import EulerSolver, FixedState, SolverConfig, jittered_rectangle_mesh
-
-    mesh = jittered_rectangle_mesh(nx, nx, JITTER, MESH_SEED)
-    mean = FixedState.from_primitive(1.0, 0.0, 0.0, 1.0, 1.4)
-    bcs = {t: mean for t in ("left", "right", "bottom", "top")}
-    solver = EulerSolver(mesh, bcs, SolverConfig(flux="roe", limiter="unlimited", gamma=1.4, precision=precision),
-                         device=device)
-    return solver, initial_state(solver, device)
-
-
-def initial_state(solver, device="cuda"):
-    import torch
-
-    x, y = solver.node_coordinates()
-    xt = torch.as_tensor(x, device=device)
-    yt = torch.as_tensor(y, device=device)
-    rng = np.random.default_rng(FIELD_SEED)
-    rho = fourier_field(xt, yt, rng, 0.5, 1.5, torch)
-    u = fourier_field(xt, yt, rng, -0.5, 0.5, torch)
-    v = fourier_field(xt, yt, rng, -0.5, 0.5, torch)
-    p = fourier_field(xt, yt, rng, 0.5, 1.5, torch)
-    e = p / 0.4 + 0.5 * rho * (u * u + v * v)
-    return torch.stack([rho, rho * u, rho * v, e], dim=-1).contiguous()
+    return microbenchmark(nx, precision, device)
 
 
 # ----------------------------------------------------------- CPU baseline ---
@@ -121,19 +84,17 @@ def _oracle_sample_worker(args):
     nx, steps = args
     sys.path.insert(0, ROOT)
     import oracle
+    from cfd_demo_b200.workloads import GAMMA, MEAN_STATE, conserved_fields, microbenchmark_mesh
     from oracle.physics import FixedState
 
-    om = oracle.mesh.perturbed_mesh(nx, nx, JITTER, MESH_SEED)  # same vertices as jittered_rectangle_mesh
-    mean = FixedState.from_primitive(1.0, 0.0, 0.0, 1.0, 1.4)
+    m = microbenchmark_mesh(nx)
+    om = oracle.mesh.TriangleMesh(np.array(m.vertices), np.array(m.elements),
+                                  {k: np.array(v) for k, v in m.boundary_edges.items()})
+    mean = FixedState.from_primitive(*MEAN_STATE, GAMMA)
     s = oracle.OracleSolver(om, {t: mean for t in ("left", "right", "bottom", "top")}, flux="roe",
-                            limiter="unlimited", gamma=1.4)
+                            limiter="unlimited", gamma=GAMMA)
     x, y = s.node_coordinates()
-    rng = np.random.default_rng(FIELD_SEED)
-    rho = fourier_field(x, y, rng, 0.5, 1.5, np)
-    u = fourier_field(x, y, rng, -0.5, 0.5, np)
-    v = fourier_field(x, y, rng, -0.5, 0.5, np)
-    p = fourier_field(x, y, rng, 0.5, 1.5, np)
-    q = oracle.primitive_to_conserved(rho, u, v, p, 1.4)
+    q = conserved_fields(x, y, np)
     dt = s.time_step(q)
     q, _ = s.step(q, dt)
     t0 = time.perf_counter()
@@ -256,10 +217,14 @@ def _barrier(world: int) -> None:
     torch.cuda.synchronize()
 
 
-def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: bool = True, sampler=None) -> dict:
+def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: bool = True, sampler=None,
+                min_seconds: float = 1.0, max_repeats: int = 200) -> dict:
     """Advance the resident state `warmup` + `steps` RK3 steps (device CFL dt,
     device run-loop control); time the `steps` with CUDA events on the
-    launching stream, and each stage launch separately."""
+    launching stream, and each stage launch separately. The block of exactly
+    `steps` steps is timed back to back `repeats` times (the same count on
+    every rank), enough blocks for the clock samples to span `min_seconds`;
+    each block is bracketed by a barrier and a device synchronisation."""
     import ctypes as C
 
     import torch
@@ -284,26 +249,41 @@ def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: b
         _native.check(lib.cfd_rk3_finish(ptr, sp))
         _native.check(lib.cfd_run_control(ptr, sp))
 
+    def block():
+        evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)] for _ in range(steps)]
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _barrier(world)
+        start.record(stream)
+        for i in range(steps):
+            one_step(evs[i] if stage_events else None)
+        stop.record(stream)
+        _barrier(world)
+        return start.elapsed_time(stop), [sum(evs[i][k][0].elapsed_time(evs[i][k][1]) for i in range(steps))
+                                          for k in range(3)]
+
     for _ in range(warmup):
         one_step()
-    _barrier(world)
     if sampler is not None:
         sampler.mark_start()
-    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)] for _ in range(steps)]
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for i in range(steps):
-        one_step(evs[i] if stage_events else None)
-    stop.record(stream)
-    _barrier(world)
+    totals, stages = [], []
+    t, sm = block()
+    totals.append(t)
+    stages.append(sm)
+    repeats = min(max_repeats, max(1, math.ceil(min_seconds * 1e3 / max(t, 1e-3))))
+    repeats = int(max_over_ranks([repeats], world, torch.device("cuda", torch.cuda.current_device()))[0])
+    for _ in range(repeats - 1):
+        t, sm = block()
+        totals.append(t)
+        stages.append(sm)
     if sampler is not None:
         sampler.mark_end()
-    total_ms = start.elapsed_time(stop)
-    stage_ms = [sum(evs[i][k][0].elapsed_time(evs[i][k][1]) for i in range(steps)) for k in range(3)]
     c = solver._read(ws.control, _native.CfdControl)
     if c.status != _native.RUN_ACTIVE:
         raise RuntimeError(f"run-loop status {c.status} during the benchmark")
-    return {"total_ms": total_ms, "stage_ms": stage_ms, "launches_per_step": 6, "time": c.time, "steps_done": c.steps}
+    med = int(np.argsort(totals)[len(totals) // 2])
+    return {"total_ms": totals[med], "stage_ms": stages[med], "block_ms": totals, "repeats": repeats,
+            "launches_per_step": 6, "time": c.time, "steps_done": c.steps,
+            "flux_integral": np.array(c.flux_integral[:])}
 
 
 def l1_density(solver, qa, qb) -> float:
@@ -365,6 +345,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         else:
             r = timed_steps(solver, steps, warmup, world)
         r["state"] = solver.download(solver.state_tensor())
+        # conservation defect over the whole run: final - initial integral + boundary flux
+        r["defect"] = solver.integrate(r["state"]) - solver.integrate(q0) + r["flux_integral"]
         results[name] = r
 
     # max over ranks of the timed region
@@ -406,6 +388,9 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                          "peak_source": peak_kind, "algorithmic_bytes_per_element_step": sum(sb)},
         }
     l1 = l1_density(fp32, results["fp32_mixed"]["state"], results["fp64"]["state"])
+    linf = float(np.abs(results["fp32_mixed"]["state"][..., 0] - results["fp64"]["state"][..., 0]).max())
+    conservation = {n: {"mass_defect": float(results[n]["defect"][0]), "energy_defect": float(results[n]["defect"][3]),
+                        "time": results[n]["time"], "steps": results[n]["steps_done"]} for n in ("fp32_mixed", "fp64")}
     state_bytes = q0.numel() * 8
     line = {
         "metric": METRIC,
@@ -439,6 +424,16 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                  "stage_ms": out["fp64"]["stage_ms"], "roofline": out["fp64"]["roofline"], "dtype": "f64"},
         "fp32_over_fp64": out["fp32_mixed"]["value"] / out["fp64"]["value"],
         "l1_rho_vs_fp64": l1,
+        "linf_rho_vs_fp64": linf,
+        "conservation": conservation,
+        "precision_note": "FP32-mixed and FP64 states after the same number of steps, each with its own device CFL "
+                          "steps (end times in `conservation`); defects = final - initial integral + time-integrated "
+                          "boundary flux",
+        "timing": {"repeats": results["fp32_mixed"]["repeats"], "block_steps": steps,
+                   "block_ms_fp32_mixed": [round(v, 4) for v in results["fp32_mixed"]["block_ms"]],
+                   "note": "each block times exactly `steps` RK3 steps (barrier + synchronise on both sides); "
+                           "value and ms_per_step from the median block; blocks repeat until the clock samples "
+                           "span >= 1 s"},
         "e2e": {"value": world * dof * e2e_steps / e2e_s, "unit": "DOF-steps/s",
                 "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": (state_bytes + 104 * e2e_steps) / e2e_steps,
                 "api": "EulerSolver.run(pinned host (Np,K,4) float64 state, t_K) -> RunResult with host state",

@@ -20,6 +20,7 @@ RUN_ACTIVE, RUN_DONE, RUN_BAD_DT, RUN_REJECTED = 0, 1, -1, -2
 NOALLOC_MAX_ELEMENTS = 16384  # CFD_NOALLOC_MAX_ELEMENTS of include/cfd_b200.h
 ADJ_HOLD_THETA = 1  # CFD_ADJ_HOLD_THETA
 LIMIT_LIST_HEADER = 16  # CFD_LIMIT_LIST_HEADER
+ABI_VERSION = 2  # CFD_ABI_VERSION
 
 _p = C.c_void_p
 _i32 = C.c_int32
@@ -55,7 +56,8 @@ class CfdControl(C.Structure):
 class CfdSolver(C.Structure):
     _fields_ = [("mesh", CfdMesh), ("flux", _i32), ("limiter", _i32), ("precision", _i32), ("max_rejections", _i32),
                 ("gamma", _f64), ("cfl", _f64), ("averages", _p), ("element_aux", _p), ("acc", _p),
-                ("report", _p), ("control", _p), ("block_size", _i32), ("variant", _i32), ("limit_list", _p)]
+                ("report", _p), ("control", _p), ("block_size", _i32), ("variant", _i32), ("limit_list", _p),
+                ("troubled_flags", _p)]
 
 
 SIZES = {"CfdMesh": C.sizeof(CfdMesh), "CfdStageAcc": C.sizeof(CfdStageAcc),
@@ -111,7 +113,7 @@ def load(path: str | None = None):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.cfd_abi_version() != 1:
+    if lib.cfd_abi_version() != ABI_VERSION:
         raise RuntimeError("libcfd_b200.so ABI version mismatch; rebuild it.")
     if path == LIB_PATH:
         _lib = lib

@@ -3,15 +3,19 @@
     python -m cfd_demo_b200.build          # or __graft_entry__.build()
 
 Steps: (1) print the degree-4 reference-triangle tables as compile-time
-constants into ``csrc/tables.cuh``; (2) compile ``csrc/*.cu`` with nvcc for
-``sm_100a`` into ``cfd_demo_b200/libcfd_b200.so`` (in-tree, so it travels with
-the repository snapshot). No CUDA device is needed to build.
+constants into ``csrc/tables.cuh``; (2) compile the objects with nvcc for
+``sm_100a`` in parallel — ``kernels.cu`` (limiter, adjoint, small kernels and
+the C ABI) and ``stage_inst.cu`` once per precision x mode of the fused stage
+kernels — into ``_build/``, each rebuilt only when its inputs change; (3) link
+them into ``cfd_demo_b200/libcfd_b200.so`` (in-tree, so it travels with the
+repository snapshot). No CUDA device is needed to build.
 """
 
 from __future__ import annotations
 
 import hashlib
 import os
+from concurrent.futures import ThreadPoolExecutor
 import shutil
 import subprocess
 import sys
@@ -23,10 +27,15 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcfd_b200.so")
-SOURCES = ["kernels.cu"]
+BUILD_DIR = os.path.join(HERE, "_build")
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
-    "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v",
+    "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
+]
+# (object name, source, extra defines)
+OBJECTS = [("kernels", "kernels.cu", [])] + [
+    (f"stage_{prec}_{mode}", "stage_inst.cu", [f"-DCFD_STAGE_PREC={p}", f"-DCFD_STAGE_MODE={m}"])
+    for p, prec in enumerate(("f64", "f32")) for m, mode in enumerate(("rhs", "limited", "unlimited"))
 ]
 
 
@@ -70,56 +79,88 @@ def generate_tables() -> str:
         _array("P1MID", ref.p1_midpoint), _array("LINBASIS", ref.linear_midpoint_basis),
         "}}  // namespace cfd::tab\n",
         "namespace cfd { namespace ctab {  // the same tables in the constant bank (warp-uniform runtime index)\n",
-        _array("DR", ref.dr).replace("__device__ constexpr", "__constant__"),
-        _array("DS", ref.ds).replace("__device__ constexpr", "__constant__"),
-        _array("LIFT", ref.lift).replace("__device__ constexpr", "__constant__"),
-        _array("DR32", ref.dr, "float").replace("__device__ constexpr", "__constant__"),
-        _array("DS32", ref.ds, "float").replace("__device__ constexpr", "__constant__"),
-        _array("LIFT32", ref.lift, "float").replace("__device__ constexpr", "__constant__"),
-        _array("AVG_W", w / w.sum()).replace("__device__ constexpr", "__constant__"),
-        _array("FACE_NODES", ref.face_nodes, "int").replace("__device__ constexpr", "__constant__"),
-        _array("FACE_W", ref.face_weights[0]).replace("__device__ constexpr", "__constant__"),
+        _array("DR", ref.dr).replace("__device__ constexpr", "static __constant__"),
+        _array("DS", ref.ds).replace("__device__ constexpr", "static __constant__"),
+        _array("LIFT", ref.lift).replace("__device__ constexpr", "static __constant__"),
+        _array("DR32", ref.dr, "float").replace("__device__ constexpr", "static __constant__"),
+        _array("DS32", ref.ds, "float").replace("__device__ constexpr", "static __constant__"),
+        _array("LIFT32", ref.lift, "float").replace("__device__ constexpr", "static __constant__"),
+        _array("AVG_W", w / w.sum()).replace("__device__ constexpr", "static __constant__"),
+        _array("FACE_NODES", ref.face_nodes, "int").replace("__device__ constexpr", "static __constant__"),
+        _array("FACE_W", ref.face_weights[0]).replace("__device__ constexpr", "static __constant__"),
         "}}  // namespace cfd::ctab\n",
     ]
     assert np.allclose(ref.face_weights, ref.face_weights[0][None]), "faces share one GLL rule"
     return "".join(text)
 
 
-def _digest(paths) -> str:
+def _digest(paths, extra=()) -> str:
     h = hashlib.sha256()
     for p in paths:
         with open(p, "rb") as f:
             h.update(f.read())
-    h.update(" ".join(NVCC_FLAGS).encode())
+    h.update(" ".join([*NVCC_FLAGS, *extra]).encode())
     return h.hexdigest()
 
 
+def _nvcc() -> str:
+    return shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+
+
+def _compile(name: str, source: str, defines: list[str], headers: list[str], force: bool) -> tuple[str, bool, str]:
+    """Compile one object unless its digest (sources + flags) is unchanged."""
+    obj = os.path.join(BUILD_DIR, name + ".o")
+    stamp = obj + ".sha256"
+    digest = _digest([os.path.join(CSRC, source), *headers], defines)
+    if not force and os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == digest:
+        return obj, False, ""
+    cmd = [_nvcc(), *NVCC_FLAGS, *defines, f"-I{INCLUDE}", f"-I{CSRC}", "-c", os.path.join(CSRC, source),
+           "-o", obj + ".tmp"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        sys.stderr.write(proc.stdout + proc.stderr)
+        raise RuntimeError(f"nvcc failed ({proc.returncode}): {' '.join(cmd)}")
+    os.replace(obj + ".tmp", obj)
+    with open(stamp, "w") as f:
+        f.write(digest)
+    with open(obj + ".ptxas.txt", "w") as f:
+        f.write(proc.stderr)
+    return obj, True, proc.stderr
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Generate the tables and compile the library if any input changed."""
+    """Generate the tables, compile the changed objects in parallel and link
+    the library if any object changed."""
     tables = os.path.join(CSRC, "tables.cuh")
     text = generate_tables()
     if not os.path.exists(tables) or open(tables).read() != text:
         with open(tables, "w") as f:
             f.write(text)
-    inputs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".inc")))
-    inputs.append(os.path.join(INCLUDE, "cfd_b200.h"))
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    headers = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc")))
+    headers.append(os.path.join(INCLUDE, "cfd_b200.h"))
+    with ThreadPoolExecutor(max_workers=min(len(OBJECTS), os.cpu_count() or 1)) as pool:
+        results = list(pool.map(lambda o: _compile(*o, headers, force), OBJECTS))
+    objs = [r[0] for r in results]
     stamp = LIB + ".sha256"
-    digest = _digest(inputs)
-    if not force and os.path.exists(LIB) and os.path.exists(stamp) and open(stamp).read() == digest:
-        return LIB
-    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    cmd = [nvcc, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
-    proc = subprocess.run(cmd, capture_output=True, text=True)
-    if proc.returncode != 0:
-        sys.stderr.write(proc.stdout + proc.stderr)
-        raise RuntimeError(f"nvcc failed ({proc.returncode}): {' '.join(cmd)}")
+    digest = _digest(objs)
+    if any(r[1] for r in results) or force or not os.path.exists(LIB) or not os.path.exists(stamp) \
+            or open(stamp).read() != digest:
+        cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB + ".tmp"]
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            sys.stderr.write(proc.stdout + proc.stderr)
+            raise RuntimeError(f"nvcc link failed ({proc.returncode}): {' '.join(cmd)}")
+        os.replace(LIB + ".tmp", LIB)
+        with open(stamp, "w") as f:
+            f.write(digest)
     with open(os.path.join(HERE, "ptxas_report.txt"), "w") as f:
-        f.write(proc.stderr)
+        for name, _, _ in OBJECTS:
+            with open(os.path.join(BUILD_DIR, name + ".o.ptxas.txt")) as g:
+                f.write(g.read())
     if verbose:
-        sys.stdout.write(proc.stderr)
-    os.replace(LIB + ".tmp", LIB)
-    with open(stamp, "w") as f:
-        f.write(digest)
+        for r in results:
+            sys.stdout.write(r[2])
     return LIB
 
 

@@ -212,27 +212,3 @@ def node_coordinates(mesh: TriangleMesh, r: np.ndarray, s: np.ndarray):
     w = np.stack([-(r + s) / 2, (1 + r) / 2, (1 + s) / 2], axis=-1)
     p = np.einsum("nv,kvd->nkd", w, c)
     return p[..., 0], p[..., 1]
-
-
-def pair_face_nodes(mesh, connectivity, x, y, face_nodes, relative_tolerance: float = 1e-9) -> np.ndarray:
-    """Neighbour node coinciding with each face node, (3, Nfp, K), the node
-    itself on boundary faces (mesh.py:254-291). Vectorised: each own face node
-    is compared with every node of the neighbour's face."""
-    nf, nfp = face_nodes.shape
-    k = mesh.num_elements
-    partner = np.broadcast_to(face_nodes[:, :, None], (nf, nfp, k)).copy()
-    scale = element_geometry(mesh).edge_length
-    for f in range(nf):
-        el = np.flatnonzero(connectivity.neighbor_element[:, f] >= 0)
-        if el.size == 0:
-            continue
-        nb = connectivity.neighbor_element[el, f]
-        cand = face_nodes[connectivity.neighbor_face[el, f]]  # (n, Nfp)
-        own = np.stack([x[face_nodes[f]][:, el], y[face_nodes[f]][:, el]], axis=-1)  # (Nfp, n, 2)
-        oth = np.stack([x[cand.T, nb[None]], y[cand.T, nb[None]]], axis=-1)
-        dist = np.hypot(own[:, None, :, 0] - oth[None, :, :, 0], own[:, None, :, 1] - oth[None, :, :, 1])
-        best = dist.argmin(axis=1)
-        if np.any(np.take_along_axis(dist, best[:, None], axis=1)[:, 0] > relative_tolerance * scale[el, f][None]):
-            raise ValueError("Neighboring face nodes do not coincide; the mesh is not conforming.")
-        partner[f][:, el] = np.take_along_axis(cand.T, best, axis=0)
-    return partner

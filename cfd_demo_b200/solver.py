@@ -122,6 +122,8 @@ class Workspace:
         self.small_i = torch.zeros(max(n, 8), dtype=torch.int32, device=dev)
         # the two-pass limiter's counters and element list
         self.limit_list = torch.zeros(_native.LIMIT_LIST_HEADER + ops.ld, dtype=torch.int32, device=dev)
+        # per-stage troubled-cell indicator, written only when recording is on
+        self.flags = torch.zeros((3, ops.ld), dtype=torch.uint8, device=dev)
 
 
 class EulerSolver:
@@ -194,6 +196,20 @@ class EulerSolver:
     def set_block_size(self, block_size: int) -> None:
         self._struct.block_size = int(block_size)
         self._graphs.clear()
+
+    def record_troubled_flags(self, enable: bool = True) -> None:
+        """Have the limiter write its per-element troubled-cell indicator
+        (limiting.py:147-151 of CFD-demo) on every call: stage k of a step
+        writes row k-1 of :meth:`troubled_flags`, :meth:`limit` row 0."""
+        self._struct.troubled_flags = self._ws.flags.data_ptr() if enable else None
+        self._graphs.clear()
+
+    def troubled_flags(self) -> np.ndarray:
+        """(3, K) bool: the troubled-cell indicator of the last step's three
+        stages (row 0 after :meth:`limit`); needs :meth:`record_troubled_flags`."""
+        if not self._struct.troubled_flags:
+            raise RuntimeError("troubled-flag recording is off; call record_troubled_flags() first.")
+        return self._ws.flags[:, : self.mesh.num_elements].cpu().numpy().astype(bool)
 
     def set_variant(self, variant: int) -> None:
         """Select the stage-kernel variant (see CfdSolver.variant)."""
@@ -296,6 +312,20 @@ class EulerSolver:
         _native.check(self._lib.cfd_limit(C.byref(self._struct), x.data_ptr(), ws.out.data_ptr(),
                                           ws.small_i.data_ptr(), _stream()))
         return self.download(ws.out), int(ws.small_i[0].item())
+
+    def limit_with_flags(self, q) -> tuple[np.ndarray, np.ndarray]:
+        """limit() plus the troubled-cell indicator of every element, (K,) bool."""
+        ws = self._ws
+        was = self._struct.troubled_flags
+        self._struct.troubled_flags = ws.flags.data_ptr()
+        try:
+            x = self.upload(q, ws.x0)
+            _native.check(self._lib.cfd_limit(C.byref(self._struct), x.data_ptr(), ws.out.data_ptr(),
+                                              ws.small_i.data_ptr(), _stream()))
+            flags = ws.flags[0, : self.mesh.num_elements].cpu().numpy().astype(bool)
+        finally:
+            self._struct.troubled_flags = was
+        return self.download(ws.out), flags
 
     def time_step(self, q) -> float:
         """CFL time step for the state q (time_integration.py:37-41)."""

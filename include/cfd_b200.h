@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define CFD_ABI_VERSION 1
+#define CFD_ABI_VERSION 2
 
 /* error codes */
 #define CFD_OK 0
@@ -181,6 +181,9 @@ typedef struct CfdSolver {
                               runs in two passes (a light detection pass over every element,
                               then the rewrite of the troubled / non-positive ones only);
                               NULL: one pass. cfd_rk3_begin resets its counters. */
+    uint8_t* troubled_flags; /* optional [3][ld]: the troubled-cell indicator of limiting.py:147-151
+                              (1 = troubled, 0 = not) of every active element; stage k of an attempt
+                              writes row k-1, cfd_limit writes row 0. NULL: not written. */
 } CfdSolver;
 
 /* ---- library ------------------------------------------------------------- */
@@ -260,7 +263,10 @@ int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, v
  * library until the process exits); larger meshes are refused with CFD_E_ARG.
  * The call allocates nothing. Its first call on a device looks up the device
  * address of that array (cudaGetSymbolAddress), so make that first call
- * before any stream capture. All calls share the one array: calls that
+ * before any stream capture; first calls from several host threads at once
+ * are safe (the lookup is done under a lock). The address stays cached for the
+ * life of the process, so do not call this entry point on a device after a
+ * cudaDeviceReset of that device. All calls share the one array: calls that
  * overlap on the GPU (other streams, other host threads) race, and the caller
  * must serialise them.
  */

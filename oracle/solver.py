@@ -245,6 +245,24 @@ class OracleSolver:
         linear = avg[None] + np.einsum("if,fkc->ikc", ref.linear_midpoint_basis, deltas)
         return np.where(troubled[None, :, None], linear, q), troubled
 
+    def detection_ratios(self, q, avg):
+        """The troubled-cell test of limiting.py:141-151 as one number per
+        element: the largest excess / threshold over the three face midpoints
+        and the detection components (troubled exactly when it exceeds one;
+        inf where a threshold is zero and the excess is not). A ratio within
+        round-off of one marks a decision that round-off can flip."""
+        ref = self.reference
+        diff = self._neighbor_averages(avg) - avg[None]
+        paired = np.take_along_axis(diff, self.partner_face[..., None], axis=0)
+        scaled = NEIGHBOR_FACTOR * (self.alpha[..., None] * diff + self.beta[..., None] * paired)
+        trace = q[ref.face_midpoint_nodes] - avg[None]
+        comp = list(DETECTION_COMPONENTS)
+        excess = np.abs(_minmod2(trace, scaled) - trace)[..., comp]
+        thresh = DETECTION_TOLERANCE * np.abs(avg[:, comp])[None]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = np.where(thresh > 0, excess / thresh, np.where(excess > 0, np.inf, 0.0))
+        return ratio.max(axis=(0, 2))
+
     def positivity_limit(self, q, avg):
         """limiting.py:166-200."""
         g = self.gamma
@@ -292,13 +310,16 @@ class OracleSolver:
             lam = np.sqrt(u * u + v * v) + sound_speed(rho, p, self.gamma)
         return float(self.cfl * np.min(self.dt_geometry / np.max(lam, axis=0)))
 
-    def step(self, q, dt, *, record=None):
+    def step(self, q, dt, *, record=None, ratios=None):
         """time_integration.py:44-84. ``record``, if a list, receives the
-        troubled flags of each stage."""
+        troubled flags of each stage; ``ratios``, if a list, each stage's
+        detection_ratios of its state before limiting."""
         q = self._as_state(q)
         g = self.gamma
 
         def lim(u):
+            if ratios is not None:
+                ratios.append(self.detection_ratios(u, np.einsum("i,ikc->kc", self.avg_weights, u)))
             u, avg, count, flags = self.apply_limiters(u)
             if record is not None:
                 record.append(flags)

@@ -1,13 +1,13 @@
 """Generate the golden fixtures of the CFD-demo hot path from the reference's
 own source.
 
-Run in a container that has the CFD-demo source tree (default
-``/root/reference``) but no JAX: ``numpy_jax.install()`` puts a NumPy stand-in
+Run in a container that has the CFD-demo source tree (its path is the
+required ``--reference`` argument) but no JAX: ``numpy_jax.install()`` puts a NumPy stand-in
 for ``jax`` in ``sys.modules`` and the reference's modules are imported and
 called unchanged. The outputs are small ``.npz`` files beside this script;
 the tests read them on machines without the reference.
 
-    python tests/golden/make_golden.py [--reference PATH] [--only NAME ...]
+    python tests/golden/make_golden.py --reference PATH [--only NAME ...]
 
 Fixtures (all float64 unless noted):
   element.npz      reference-triangle tables
@@ -19,6 +19,10 @@ Fixtures (all float64 unless noted):
   sod_100x10.npz  run() of the 100x10 Sod tube to t = 0.2 (rusanov/minmod),
                    with per-step dt, report and per-stage troubled counts and
                    the troubled flags of the first 25 steps
+  sod_100x10_flags.npz  the same run's troubled flags at every stage of every
+                   step (bit-packed, each stage XOR the previous one) and its
+                   borderline detection decisions: every element whose
+                   largest excess / threshold ratio lies within 1e-3 of one
 """
 
 from __future__ import annotations
@@ -336,15 +340,78 @@ def gen_sod_100x10(ref):
     return instrumented_run(ref, case.solver, case.initial_state, case.final_time, flag_steps=25)
 
 
+def gen_sod_100x10_flags(ref):
+    """Every stage's troubled flags of the config-0 run, plus the decisions
+    that round-off can flip: the detection of limiting.py:141-151 evaluated
+    with the reference's own helpers on the stage's arguments, giving each
+    element's largest excess / threshold ratio (flag = ratio > 1)."""
+    lim = ref["limiting"]
+    original = lim.troubled_cell_limit
+    stage_rows = []
+
+    def recording(q, averages, operators, phi):
+        out_q, flags = original(q, averages, operators, phi)
+        differences = lim.neighbor_averages(averages, operators) - averages[None]
+        paired = np.take_along_axis(differences, np.asarray(operators.partner_face)[..., None], axis=0)
+        scaled = lim.NEIGHBOR_FACTOR * (np.asarray(operators.alpha)[..., None] * differences
+                                        + np.asarray(operators.beta)[..., None] * paired)
+        trace = q[np.asarray(operators.midpoint_nodes)] - averages[None]
+        comps = np.asarray(lim.DETECTION_COMPONENTS)
+        excess = np.abs(lim._minmod(trace, scaled) - trace)[..., comps]
+        threshold = lim.DETECTION_TOLERANCE * np.abs(averages[:, comps])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = np.where(threshold[None] > 0, excess / threshold[None], np.where(excess > 0, np.inf, 0.0))
+        worst = ratio.max(axis=(0, 2))
+        assert np.array_equal(worst > 1.0, np.asarray(flags)), "ratio test disagrees with the reference's flags"
+        stage_rows.append((np.asarray(flags).copy(), worst))
+        return out_q, flags
+
+    case = ref["cases"].sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")
+    solver = case.solver
+    orig_step = solver._step
+    attempts = []
+
+    def step_capture(*args):
+        stage_rows.clear()
+        out = orig_step(*args)
+        attempts.append((bool(out[1].admissible), list(stage_rows)))
+        return out
+
+    lim.troubled_cell_limit = recording
+    solver._step = step_capture
+    try:
+        solver.run(case.initial_state, case.final_time)
+    finally:
+        lim.troubled_cell_limit = original
+        solver._step = orig_step
+    flags, border = [], []
+    for ok, rows in attempts:
+        if not ok:
+            continue
+        n = len(flags)
+        flags.append(np.stack([r[0] for r in rows]))
+        for k, (_, worst) in enumerate(rows):
+            for e in np.nonzero(np.abs(worst - 1.0) <= 1e-3)[0]:
+                border.append((n, k, int(e), float(worst[e])))
+    flags = np.stack(flags).astype(np.uint8)  # (steps, 3, K)
+    seq = flags.reshape(-1, flags.shape[-1])
+    delta = seq.copy()
+    delta[1:] ^= seq[:-1]
+    border = np.asarray(border, dtype=np.float64).reshape(-1, 4)
+    print(f"  {flags.shape[0]} steps, {int(flags.sum())} troubled decisions, {len(border)} borderline")
+    return {"flags_delta_packed": np.packbits(delta, axis=-1), "flags_shape": np.asarray(flags.shape),
+            "border": border}
+
+
 GENERATORS = {
     "element": gen_element, "pointwise": gen_pointwise, "rhs": gen_rhs, "limit": gen_limit, "step": gen_step,
-    "sod_short": gen_sod_short, "sod_100x10": gen_sod_100x10,
+    "sod_short": gen_sod_short, "sod_100x10": gen_sod_100x10, "sod_100x10_flags": gen_sod_100x10_flags,
 }
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the CFD-demo source tree")
     ap.add_argument("--only", nargs="*", default=None)
     args = ap.parse_args()
     ref = load_reference(args.reference)

@@ -42,3 +42,20 @@ def boundary_specs(data: dict, prefix: str) -> dict:
 def unpack_flags(data: dict) -> np.ndarray:
     shape = tuple(int(v) for v in data["troubled_flags_shape"])
     return np.unpackbits(data["troubled_flags_packed"], axis=-1, count=shape[-1]).astype(bool).reshape(shape)
+
+
+def flag_history() -> np.ndarray:
+    """(steps, 3, K) bool: the reference's troubled flags at every stage of
+    the config-0 Sod run (sod_100x10_flags.npz stores each stage XOR the
+    previous one, bit-packed)."""
+    data = load("sod_100x10_flags")
+    shape = tuple(int(v) for v in data["flags_shape"])
+    delta = np.unpackbits(data["flags_delta_packed"], axis=-1, count=shape[-1]).astype(bool)
+    return np.logical_xor.accumulate(delta, axis=0).reshape(shape)
+
+
+def borderline_decisions() -> dict:
+    """(step, stage, element) -> the reference's largest excess / threshold
+    ratio there, for every decision of the config-0 run within 1e-3 of one."""
+    rows = load("sod_100x10_flags")["border"]
+    return {(int(n), int(k), int(e)): float(r) for n, k, e, r in rows}

@@ -1,0 +1,201 @@
+"""Troubled-cell flags element by element, and where the config-0 Sod run
+leaves the reference's trajectory.
+
+The reference decides each element's troubled flag at limiting.py:147-151:
+|minmod(trace, nu Delta) - trace| > 1e-10 |avg| at any face midpoint, for
+density or energy. The CUDA limiter writes that indicator per element when
+asked (CfdSolver.troubled_flags); here it is compared bit for bit with the
+flags the reference's own source produced:
+
+  * the four limit.npz cases x five limiters, through cfd_limit, in both the
+    one-pass and the two-pass form of the limiter;
+  * every stage of every step of the Sod 100x10 run (3186 steps x 3 stages,
+    sod_100x10_flags.npz), marched along the reference's dt sequence;
+  * the same case through run() with the device's own CFL step.
+
+The reference's trajectory holds decisions whose excess / threshold ratio
+lies within a few 1e-6 of one (sod_100x10_flags.npz lists every decision
+within 1e-3 of one). Any implementation whose arithmetic is not bit-identical
+to the reference's (including JAX/XLA against NumPy) can decide those either
+way; the tests therefore find the first stage whose flags differ at all,
+require every differing element there to be one of the reference's listed
+borderline decisions, and report the margin.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.golden_io import LIMITERS, borderline_decisions, case_prefixes, flag_history, load
+from tests.gpu_helpers import make_solver, rel_err
+
+pytestmark = pytest.mark.gpu
+
+# A decision that round-off can flip: the reference's ratio lies this close to one.
+BORDER = 1e-3
+
+
+@pytest.mark.parametrize("two_pass", [True, False])
+@pytest.mark.parametrize("prefix", case_prefixes(load("limit")))
+@pytest.mark.parametrize("limiter", LIMITERS)
+def test_limiter_flags_are_the_references_bit_for_bit(prefix, limiter, two_pass):
+    g = load("limit")
+    s = make_solver(g, prefix, limiter=limiter)
+    if not two_pass:
+        s.native.limit_list = None
+    limited, flags = s.limit_with_flags(g[f"{prefix}/q"])
+    if limiter == "unlimited":
+        assert not flags.any()
+    else:
+        assert np.array_equal(flags, g[f"{prefix}/troubled/{limiter}"]), np.nonzero(
+            flags != g[f"{prefix}/troubled/{limiter}"])
+    assert rel_err(limited, g[f"{prefix}/limited/{limiter}"]) <= 1e-12
+
+
+def _sod_case():
+    from cfd_demo_b200 import sod_shock_tube
+
+    g = load("sod_100x10")
+    case = sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")
+    assert np.array_equal(case.initial_state, g["initial_state"])
+    return case, g
+
+
+def _l1_rho(solver, q, ref):
+    w = solver.reference.cell_weights
+    jac = np.asarray(solver.geometry.jacobian)
+    return float(np.einsum("i,ik,k->", w, np.abs(q[..., 0] - ref[..., 0]), jac) / np.einsum("i,k->", w, jac))
+
+
+def _departure(n, k, gpu_flags, ref_flags, state_before, dt):
+    """The elements whose flag differs at step n, stage k, each with the
+    reference's ratio there and the ratio the oracle computes from the GPU's
+    own state at the start of that step."""
+    import oracle
+
+    border = borderline_decisions()
+    differ = np.nonzero(gpu_flags != ref_flags)[0]
+    osolver = oracle.sod_shock_tube(100, 10, flux="rusanov", limiter="minmod")[0]
+    ratios = []
+    osolver.step(state_before, dt, ratios=ratios)
+    out = []
+    for e in differ:
+        out.append((int(e), border.get((n, k, int(e))), float(ratios[k][e]), bool(gpu_flags[e])))
+    return out
+
+
+def _describe(n, k, rows):
+    parts = [f"element {e}: reference ratio {'%.7f' % r if r is not None else 'not borderline'}, "
+             f"oracle on the GPU state {ro:.7f}, GPU flag {int(f)}" for e, r, ro, f in rows]
+    return f"step {n} stage {k + 1}: " + "; ".join(parts)
+
+
+def test_sod_100x10_flags_along_the_reference_dt_sequence(report):
+    """March the reference's 3186 dt values through step(): every stage's
+    flags must equal the reference's bit for bit until the first stage at
+    which they differ; there every differing element must be one of the
+    reference's borderline decisions (ratio within 1e-3 of one). Without such
+    a departure the final state agrees to 1e-10, after one to 1e-4 in L1."""
+    case, g = _sod_case()
+    hist = flag_history()
+    s = case.solver
+    s.record_troubled_flags(True)
+    q = case.initial_state
+    first = None
+    flux_integral = np.zeros(4)
+    for n, dt in enumerate(g["dt"]):
+        before = q
+        q, rep = s.step(q, float(dt))
+        assert rep.admissible
+        flux_integral += rep.boundary_flux
+        if first is not None:
+            continue
+        fl = s.troubled_flags()
+        for k in range(3):
+            if not np.array_equal(fl[k], hist[n, k]):
+                first = (n, k, _departure(n, k, fl[k], hist[n, k], before, float(dt)))
+                break
+        else:
+            assert rep.min_density == pytest.approx(float(g["step_minima"][n][0]), rel=1e-9), f"step {n}"
+    err = rel_err(q, g["state"])
+    l1 = _l1_rho(s, q, g["state"])
+    if first is None:
+        report(f"Sod 100x10 along the reference dt sequence: flags of all {3 * len(g['dt'])} stages bit-exact; "
+               f"final state rel err {err:.2e}, L1(rho) {l1:.2e}")
+        assert err <= 1e-10
+        np.testing.assert_allclose(flux_integral, g["boundary_flux_integral"], rtol=1e-10, atol=1e-13)
+        return
+    n, k, rows = first
+    report(f"Sod 100x10 along the reference dt sequence: flags bit-exact for {3 * n + k} stages, first difference at "
+           + _describe(n, k, rows) + f"; final state rel err {err:.2e}, L1(rho) {l1:.2e}")
+    for e, r, _, _ in rows:
+        assert r is not None and abs(r - 1.0) <= BORDER, (n, k, e, r)
+    assert l1 <= 1e-4
+
+
+def test_sod_100x10_run_departs_only_at_a_borderline_decision(report):
+    """run() with the device's CFL step, one attempt per graph replay: each
+    step's dt is compared with the reference's, each stage's flags with the
+    reference's, until the first stage whose flags differ. Up to there the
+    dt values agree to 1e-13 relative (bit-equal counts are reported); at the
+    departure every differing element is one of the reference's borderline
+    decisions. Without a departure the final state agrees to 1e-10. The same
+    run through run() (chunked graphs) must give the identical final state:
+    the path is deterministic."""
+    from cfd_demo_b200 import _native
+
+    case, g = _sod_case()
+    hist = flag_history()
+    s = case.solver
+    s.record_troubled_flags(True)
+    s.begin_run(case.initial_state, case.final_time)
+    c = s.advance(0, graph=False)
+    first = None
+    equal_dt = 0
+    max_dt_rel = 0.0
+    n = 0
+    while c.status == _native.RUN_ACTIVE:
+        dt = c.dt
+        before = s.download(s.state_tensor()) if first is None else None
+        c2 = s.advance(1)
+        if c2.steps == c.steps:  # a rejected attempt (none in this case)
+            c = c2
+            continue
+        if first is None and n < len(g["dt"]):
+            ref_dt = float(g["dt"][n])
+            equal_dt += dt == ref_dt
+            max_dt_rel = max(max_dt_rel, abs(dt - ref_dt) / ref_dt)
+            fl = s.troubled_flags()
+            for k in range(3):
+                if not np.array_equal(fl[k], hist[n, k]):
+                    first = (n, k, _departure(n, k, fl[k], hist[n, k], before, dt))
+                    break
+        n += 1
+        c = c2
+    assert c.status == _native.RUN_DONE
+    final = s.download(s.state_tensor())
+    l1 = _l1_rho(s, final, g["state"])
+    steps_to = first[0] if first else n
+    head = (f"Sod 100x10 run(): {n} steps (ref {int(g['steps'])}); dt bit-equal in {equal_dt} of the first "
+            f"{steps_to} steps, max rel difference {max_dt_rel:.1e}; ")
+    if first is None:
+        report(head + f"flags bit-exact at every stage; final L1(rho) {l1:.2e}")
+        assert rel_err(final, g["state"]) <= 1e-10
+    else:
+        nn, k, rows = first
+        report(head + "first flag difference at " + _describe(nn, k, rows) + f"; final L1(rho) vs ref {l1:.2e}")
+        for e, r, _, _ in rows:
+            assert r is not None and abs(r - 1.0) <= BORDER, (nn, k, e, r)
+        assert l1 <= 1e-4
+    assert max_dt_rel <= 1e-13
+    assert abs(n - int(g["steps"])) <= 3
+    # determinism: the chunked-graph run() lands on the same bits
+    res = s.run(case.initial_state, case.final_time)
+    assert res.steps == n and res.rejected_steps == 0
+    assert np.array_equal(res.state, final), np.abs(res.state - final).max()
+    assert res.time == pytest.approx(0.2, abs=1e-15)
+    assert res.min_density == pytest.approx(float(g["min_density"]), rel=1e-6)
+    assert res.min_pressure >= 1e-13 * (1.0 - 1e-9)
+    defect = s.integrate(res.state) - s.integrate(case.initial_state) + res.boundary_flux_integral
+    assert np.abs(defect).max() <= 1e-12

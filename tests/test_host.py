@@ -203,7 +203,8 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) <= set(_native.exported_symbols()) | {"cfd_struct_sizes"}
-    assert lib.cfd_abi_version() == 1
+    assert lib.cfd_abi_version() == _native.ABI_VERSION
+    assert f"#define CFD_ABI_VERSION {_native.ABI_VERSION}" in header
 
 
 def test_struct_layouts_agree_with_the_header():
