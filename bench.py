@@ -79,9 +79,10 @@ def make_workload(nx: int = NX, precision: str = "fp32_mixed", device="cuda"):
 
 # ----------------------------------------------------------- CPU baseline ---
 def _oracle_sample_worker(args):
-    """Time `steps` oracle RK3 steps (after one warm-up) on an nx x nx sample
-    of the workload; returns (elements, steps, seconds)."""
-    nx, steps = args
+    """Time RK3 steps of the oracle on an nx x nx sample of the workload: one
+    untimed warm-up step, then as many timed steps as fit in `budget_s`
+    (at least one, at most `steps`); returns (elements, steps, seconds)."""
+    nx, steps, budget_s = args
     sys.path.insert(0, ROOT)
     import oracle
     from cfd_demo_b200.workloads import GAMMA, MEAN_STATE, conserved_fields, microbenchmark_mesh
@@ -95,27 +96,43 @@ def _oracle_sample_worker(args):
                             limiter="unlimited", gamma=GAMMA)
     x, y = s.node_coordinates()
     q = conserved_fields(x, y, np)
+    w0 = time.perf_counter()
     dt = s.time_step(q)
     q, _ = s.step(q, dt)
+    per_step = time.perf_counter() - w0
+    n = max(1, min(steps, int(budget_s / max(per_step, 1e-9))))
     t0 = time.perf_counter()
-    for _ in range(steps):
+    for _ in range(n):
         dt = s.time_step(q)
         q, _ = s.step(q, dt)
-    return s.mesh.num_elements, steps, time.perf_counter() - t0
+    return s.mesh.num_elements, n, time.perf_counter() - t0
 
 
-def cpu_baseline(nx: int, steps: int, processes: int) -> dict:
+def cpu_baseline(nx: int, steps: int, processes: int, budget_s: float = 90.0) -> dict:
     """The CPU oracle (NumPy restatement of the reference) on `processes`
-    spawned workers, each timing `steps` RK3 steps of an nx x nx sample."""
+    spawned workers, each timing RK3 steps of an nx x nx sample of the
+    workload (at most `steps`, within `budget_s` of CPU time per worker). With
+    nx = 724 / sqrt(processes) the workers together hold about the
+    benchmark's K elements."""
     ctx = mp.get_context("spawn")
     with ctx.Pool(processes) as pool:
-        results = pool.map(_oracle_sample_worker, [(nx, steps)] * processes)
+        results = pool.map(_oracle_sample_worker, [(nx, steps, budget_s)] * processes)
     k = results[0][0]
+    # whole-job rate: every worker's DOF-steps over the slowest worker's time
     slowest = max(r[2] for r in results)
-    value = processes * k * NP_NODES * steps / slowest
+    value = sum(r[0] * NP_NODES * r[1] for r in results) / slowest
+    n = min(r[1] for r in results)
     return {"value": value, "unit": "DOF-steps/s", "cores": processes, "kind": "port",
-            "sample": f"{processes} process(es) x {steps} RK3 steps of a {nx}x{nx} sample of the workload "
-                      f"(K={k}, roe/unlimited), NumPy float64 oracle; {slowest:.1f} s"}
+            "sample": f"{processes} process(es), each {n}+ RK3 steps of a {nx}x{nx}-quad sample of the workload "
+                      f"(K={k} per process, {processes * k} in all; roe/unlimited, jitter 0.2h, Fourier fields), "
+                      f"NumPy float64 oracle after one warm-up step; slowest worker {slowest:.1f} s",
+            "elements_total": processes * k}
+
+
+def sample_nx(processes: int) -> int:
+    """Quads per side of each worker's sample: together the workers cover
+    about the benchmark's 724 x 724 quads."""
+    return max(8, int(round(NX / math.sqrt(max(processes, 1)))))
 
 
 # ----------------------------------------------------------------- clocks ---
@@ -444,60 +461,81 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     return line
 
 
-def run_batch(args) -> dict:
+def run_batch(args, sequential_stride: int = 1) -> dict:
     """The batching form: seeded Riemann instances of uneven size (hllc/superbee,
-    FP32-mixed) advanced together by CUDA-graph chunks of RK3 steps, against the
-    same instances advanced one at a time (EulerSolver, also graph-replayed).
-    Both arms take the same number of steps per instance (from t = 0, device
-    CFL dt, t_final = 0.15), so the ratio is of DOF-steps/s. (Run to t = 0.15,
-    some instances of this family collapse toward vacuum in the reference
-    algorithm itself and their CFL step falls below 1e-8.)"""
+    FP32-mixed) advanced together from t = 0 to t = 0.15, each with its own
+    CFL steps, against the same instances advanced one at a time
+    (EulerSolver.run, graph-replayed run loop). The batch's execution form
+    (one persistent launch per chunk, or graph chunks of the separate
+    launches) and tile shape are picked by the autotuner. The sequential arm
+    times every `sequential_stride`-th instance; the ratio is of DOF-steps/s
+    (sum over instances of K_i Np x steps_i per second of wall time)."""
     import torch
 
     from cfd_demo_b200 import EulerSolver, SolverConfig
+    from cfd_demo_b200.autotune import autotune_batch
     from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
 
     torch.cuda.set_device(0)
     cases = riemann_batch(args.batch_count, seed=0)
     cfg = SolverConfig(flux="hllc", limiter="superbee", gamma=1.4, precision="fp32_mixed")
-    steps = args.batch_steps
+    t_end = args.batch_final_time
     states = [c.initial_state for c in cases]
-    batch = BatchedEulerSolver(cases, cfg, variant=args.variant or 0, graph_chunk=steps)
-    batch.begin_run(states, args.batch_final_time)
-    batch.advance(steps)  # warm-up: captures the graph
-    batch.begin_run(states, args.batch_final_time)
+    batch = BatchedEulerSolver(cases, cfg, graph_chunk=args.batch_chunk)
+    tuned = autotune_batch(batch, states, t_end)
+    batch.run_to(states, t_end)  # warm-up: captures every chunk size's graph
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    ctl = batch.advance(steps)
+    ctl = batch.run_to(states, t_end)
     torch.cuda.synchronize()
     batched_s = time.perf_counter() - t0
     done = np.array([c.steps for c in ctl])
     sizes = np.array([c.mesh.num_elements for c in cases])
+    status = np.array([c.status for c in ctl])
     dof_steps = float((done * sizes * NP_NODES).sum())
-    nseq = min(args.batch_sequential, len(cases))
-    seq_s, seq_dof = 0.0, 0.0
-    for i in range(nseq):
+    picked = list(range(0, len(cases), sequential_stride))
+    seq_s, seq_dof, mismatched = 0.0, 0.0, []
+    for i in picked:
         c = cases[i]
-        single = EulerSolver(c.mesh, c.boundary_conditions, cfg, variant=args.variant or 0, graph_chunk=steps)
-        single.begin_run(c.initial_state, args.batch_final_time)
-        single.advance(steps)  # warm-up: captures the graph
-        single.begin_run(c.initial_state, args.batch_final_time)
+        single = EulerSolver(c.mesh, c.boundary_conditions, cfg, graph_chunk=args.batch_chunk)
+        single.set_variant(9)
+        try:
+            single.run(c.initial_state, t_end)  # warm-up
+        except Exception:  # noqa: BLE001 - an instance that stops early stops in both arms
+            pass
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        cs = single.advance(steps)
+        single.begin_run(c.initial_state, t_end)
+        chunk = 1
+        while True:
+            cs = single.advance(chunk)
+            if cs.status != 0:
+                break
+            chunk = min(2 * chunk, args.batch_chunk)
         torch.cuda.synchronize()
         seq_s += time.perf_counter() - t1
         seq_dof += cs.steps * c.mesh.num_elements * NP_NODES
-        assert cs.steps == done[i], (i, cs.steps, done[i])
+        if cs.steps != done[i] or cs.status != status[i]:
+            mismatched.append(i)
     seq_value = seq_dof / seq_s if seq_s else None
+    names = {1: "done", -1: "bad CFL step", -2: "too many rejections", 0: "active"}
     return {
-        "metric": "batched vs sequential DOF-steps/s (seeded Riemann instances)", "value": dof_steps / batched_s,
-        "unit": "DOF-steps/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32",
-        "config": {"workload": f"{len(cases)} seeded Riemann instances on [0,1]x[0,0.1], nx in 50..400, "
-                               f"ny=floor(nx/10), hllc/superbee, FP32-mixed, {steps} RK3 steps each",
-                   "elements_total": int(sizes.sum()), "instances": len(cases)},
-        "batched_seconds": batched_s, "batched_instance_steps": int(done.sum()),
-        "sequential": {"instances_timed": nseq, "seconds": seq_s, "value": seq_value},
+        "metric": "batched vs sequential DOF-steps/s (seeded Riemann instances to t = 0.15)",
+        "value": dof_steps / batched_s, "unit": "DOF-steps/s", "n_gpus": 1, "higher_is_better": True,
+        "data": "synthetic", "dtype": "f32",
+        "config": {"workload": f"{len(cases)} seeded Riemann instances on [0,1]x[0,0.1] (left/right rho, p uniform in "
+                               f"[0.1,1], u = v = 0), nx in 50..400, ny = floor(nx/10), hllc/superbee, FP32-mixed, "
+                               f"t = 0 -> {t_end}",
+                   "elements_total": int(sizes.sum()), "instances": len(cases),
+                   "execution": {"choice": list(tuned["choice"]), "attempt_chunk_ms": tuned["ms"]}},
+        "batched_seconds": batched_s, "batched_instance_steps": int(done.sum()), "max_steps": int(done.max()),
+        "instances_by_status": {names.get(int(k), str(k)): int((status == k).sum()) for k in np.unique(status)},
+        "stopped_early": [{"instance": int(i), "status": names.get(int(status[i])), "steps": int(done[i]),
+                           "time": float(ctl[i].time),
+                           "nx": int(len(np.unique(cases[i].mesh.vertices[:, 0])) - 1)}
+                          for i in np.nonzero(status != 1)[0]],
+        "sequential": {"instances_timed": len(picked), "stride": sequential_stride, "seconds": seq_s,
+                       "value": seq_value, "step_count_mismatches": mismatched},
         "speedup_vs_sequential": (dof_steps / batched_s) / seq_value if seq_value else None,
     }
 
@@ -621,16 +659,19 @@ def run_precision(args) -> dict:
 
 def run_reference(args) -> dict:
     """The reference arm: the CPU oracle (NumPy restatement of the reference's
-    own algorithm; JAX is not installed) on the host cores."""
+    own algorithm; the reference itself is JAX code that cannot be installed
+    on the box) on every host core, each worker advancing its own share-sized
+    sample of the workload."""
     procs = args.cpu_procs or os.cpu_count() or 1
-    steps = args.steps
-    base = cpu_baseline(args.ref_nx, steps, procs)
+    nx = args.ref_nx or sample_nx(procs)
+    base = cpu_baseline(nx, args.steps, procs, budget_s=args.ref_budget)
     return {
-        "metric": METRIC, "value": base["value"], "unit": "DOF-steps/s", "n_gpus": args.gpus, "steps": steps,
+        "metric": METRIC, "value": base["value"], "unit": "DOF-steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"sample of the 1M-triangle RK3 microbenchmark ({args.ref_nx}x{args.ref_nx} quads x 2), "
-                               "roe/unlimited", "flux": "roe", "limiter": "unlimited"},
+        "config": {"workload": f"1M-triangle RK3 microbenchmark split into {procs} samples of {nx}x{nx} quads x 2 "
+                               f"({base['elements_total']} elements in all), roe/unlimited", "flux": "roe",
+                   "limiter": "unlimited"},
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "DOF-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -643,7 +684,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--nx", type=int, default=NX)
-    ap.add_argument("--ref-nx", type=int, default=48)
+    ap.add_argument("--ref-nx", type=int, default=0, help="CPU sample quads per side (default: 724/sqrt(processes))")
+    ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU work per worker")
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--cpu-baseline-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -657,10 +699,11 @@ def main() -> None:
     ap.add_argument("--precision-quad", type=int, default=6)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing of the default line")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances timing of the default line")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-final-time", type=float, default=0.15)
-    ap.add_argument("--batch-sequential", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--batch-chunk", type=int, default=64, help="attempts per graph chunk of the batch run")
+    ap.add_argument("--batch-stride", type=int, default=1, help="time every n-th instance in the sequential arm")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
@@ -670,7 +713,7 @@ def main() -> None:
 
     if args.workload == "batch":
         if rank == 0:
-            print(json.dumps(run_batch(args)), flush=True)
+            print(json.dumps(run_batch(args, args.batch_stride)), flush=True)
         return
     if args.workload == "adjoint":
         if rank == 0:
@@ -689,7 +732,8 @@ def main() -> None:
     # CPU baseline first (spawned workers, before any CUDA context)
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(args.ref_nx, args.cpu_baseline_steps, args.cpu_procs or os.cpu_count() or 1)
+        procs = args.cpu_procs or os.cpu_count() or 1
+        base = cpu_baseline(args.ref_nx or sample_nx(procs), args.cpu_baseline_steps, procs, budget_s=20.0)
 
     if world > 1:
         import datetime
@@ -709,6 +753,8 @@ def main() -> None:
         line["cpu_baseline"] = base
         if world == 1 and not args.no_adjoint:
             line["adjoint"] = run_adjoint(args)
+        if world == 1 and not args.no_batch:
+            line["batch"] = run_batch(args, sequential_stride=8)
         print(json.dumps(line), flush=True)
 
 

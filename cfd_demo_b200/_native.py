@@ -36,6 +36,14 @@ class CfdMesh(C.Structure):
     ]
 
 
+class CfdMeshBuild(C.Structure):
+    _fields_ = [
+        ("num_vertices", _i32), ("num_elements", _i32), ("ld", _i32), ("num_boundary_edges", _i32),
+        ("num_tags", _i32), ("reserved", _i32), ("vertices", _p), ("elements", _p), ("boundary_edges", _p),
+        ("boundary_tag", _p), ("tag_kind", _p), ("tag_row", _p),
+    ]
+
+
 class CfdStageAcc(C.Structure):
     _fields_ = [("boundary_flux", _f64 * 4), ("min_rho_key", C.c_uint64), ("min_p_key", C.c_uint64),
                 ("dt_key", C.c_uint64), ("troubled", _i32), ("flags", _i32)]
@@ -82,11 +90,14 @@ _PROTOS = {
     "cfd_rk3_finish": (C.c_int, [_SP, _p]),
     "cfd_run_control": (C.c_int, [_SP, _p]),
     "cfd_run_init": (C.c_int, [_SP, _p, _p, _p]),
+    "cfd_batch_advance": (C.c_int, [_SP, _p, _p, _p, _i32, _p]),
     "cfd_rk3_step_noalloc": (C.c_int, [C.POINTER(CfdMesh), _i32, _i32, _i32, _f64, _f64, _p, _p, _f64, _p, _p]),
     "cfd_tape_bytes": (C.c_int64, [_i32, _i32]),
     "cfd_adjoint_work_bytes": (C.c_int64, [_i32, _i32]),
     "cfd_rk3_step_fixed": (C.c_int, [_SP, _p, _p, _p, _p, _p, _p]),
     "cfd_rk3_step_adjoint": (C.c_int, [_SP, _p, _p, _p, _p, _p, _p, _i32, _p, _p]),
+    "cfd_mesh_build_work_bytes": (C.c_int64, [_i32, _i32]),
+    "cfd_mesh_build": (C.c_int, [C.POINTER(CfdMeshBuild), C.POINTER(CfdMesh), _p, _f64, _p, C.c_int64, _p, _p]),
     "cfd_interface_flux": (C.c_int, [_i32, _i32, _p, _p, _p, _p, _f64, _p, _p]),
     "cfd_limiter_phi": (C.c_int, [_i32, _i32, _p, _p, _p]),
 }

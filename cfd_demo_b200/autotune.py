@@ -19,6 +19,11 @@ The fused stage kernel comes in ten shapes (CfdSolver.variant):
      allow)
   9  shape 8 with the face-node flux as an out-of-line call, so the eight
      unrolled face rounds share one copy of the flux code (FP32; FP64 runs 8)
+  10 shape 3 in the face-job form: the block lists the faces it owns (each
+     in-tile interior face once), deals their face nodes out to all threads,
+     evaluates each face flux once for both sides and lifts the 15 jump
+     inputs of each element from shared memory
+  11 shape 8 (staged base rows) in the face-job form
 `autotune(solver, state)` times one RK3 attempt per candidate on the solver's
 own buffers (an attempt from the same state recomputes the same step, so the
 candidates see identical work), keeps the fastest, and remembers the choice per
@@ -32,7 +37,7 @@ import math
 
 from . import _native
 
-CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (8, 0), (9, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
+CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (8, 0), (9, 0), (10, 0), (11, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
 _cache: dict = {}
 
 
@@ -78,3 +83,34 @@ def autotune(solver, state, *, repeats: int = 3, candidates=CANDIDATES, use_cach
     result = {"choice": best, "ms": times}
     _cache[key] = result
     return result
+
+
+BATCH_CANDIDATES = (("persistent", 9), ("chunks", 3), ("chunks", 8), ("chunks", 9), ("chunks", 0))
+
+
+def autotune_batch(batch, states, final_time, *, attempts: int = 16, candidates=BATCH_CANDIDATES) -> dict:
+    """Pick the faster execution form of a BatchedEulerSolver: the persistent
+    launch (its tile shape is fixed per precision) or CUDA-graph chunks of the
+    separate launches with one of the tiled shapes. Each candidate advances
+    the same states `attempts` attempts from t = 0 (after a warm-up chunk that
+    captures its graph); the batch is left set to the fastest.
+    Returns {"choice": (form, variant), "ms": {...}}."""
+    import torch
+
+    times = {}
+    for form, variant in candidates:
+        batch.persistent = form == "persistent"
+        batch.set_variant(variant)
+        batch.begin_run(states, final_time)
+        batch.advance(attempts)  # warm-up: captures the chunk's graph
+        batch.begin_run(states, final_time)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        batch.advance(attempts)
+        stop.record()
+        stop.synchronize()
+        times[f"{form}/variant{variant}"] = start.elapsed_time(stop)
+    best = min(candidates, key=lambda fv: times[f"{fv[0]}/variant{fv[1]}"])
+    batch.persistent = best[0] == "persistent"
+    batch.set_variant(best[1])
+    return {"choice": best, "ms": times}

@@ -8,8 +8,13 @@ buffers, step and rejection counts, minima, boundary-flux integral), so the
 instances march with their own CFL steps, are rejected and retried on their
 own, and stop at their own final time exactly as `EulerSolver.run` does
 (solver.py:167-216 of CFD-demo); finished instances are skipped by the kernels.
-The host replays CUDA-graph chunks of (attempt + control) and polls the loop
-states once per chunk.
+Two execution forms. ``persistent=True`` (the default): each chunk of
+attempts is ONE cooperative launch (cfd_batch_advance) whose blocks stay
+resident, loop over the tiles of every instance and step through the phases
+of each attempt with grid-wide barriers; the chunk's launch is captured in a
+CUDA graph and replayed. ``persistent=False``: CUDA-graph chunks of the
+separate launches (cfd_rk3_attempt + cfd_run_control per attempt). Either
+way the host polls the loop states once per chunk.
 
 `riemann_batch` builds the seeded benchmark family: Riemann problems on
 [0,1]x[0,0.1] strips split at x = 0.5 with left/right density and pressure
@@ -65,7 +70,8 @@ def riemann_batch(count: int = 256, seed: int = 0, nx_range=(50, 400), gamma: fl
 class BatchedEulerSolver:
     """Several independent problems with one configuration, advanced together."""
 
-    def __init__(self, cases, config: SolverConfig, *, device="cuda", graph_chunk: int = 64, variant: int = 0):
+    def __init__(self, cases, config: SolverConfig, *, device="cuda", graph_chunk: int = 64, variant: int = 0,
+                 persistent: bool = True):
         import torch
 
         if not torch.cuda.is_available():
@@ -101,6 +107,10 @@ class BatchedEulerSolver:
         self._struct = s
         self._graph_chunk = int(graph_chunk)
         self._graphs: dict = {}
+        self.persistent = bool(persistent)
+        if self.persistent:  # the per-device lookup of the resident grid, outside any capture
+            _native.check(self._lib.cfd_batch_advance(C.byref(s), self._ws.x0.data_ptr(), self._ws.x1.data_ptr(),
+                                                      self._ws.stage.data_ptr(), 0, _stream()))
 
     @property
     def num_instances(self) -> int:
@@ -117,6 +127,18 @@ class BatchedEulerSolver:
     def set_variant(self, variant: int) -> None:
         self._struct.variant = int(variant)
         self._graphs.clear()
+
+    def run_to(self, states, final_time, *, max_chunk: int | None = None) -> list:
+        """Advance every instance from t = 0 until each has ended (done, or
+        stopped by a bad CFL step or too many rejections, without raising);
+        returns the loop states (CfdControl) of all instances."""
+        self.begin_run(states, final_time)
+        chunk, cap = 1, max_chunk or self._graph_chunk
+        while True:
+            ctl = self.advance(chunk)
+            if all(c.status != _native.RUN_ACTIVE for c in ctl):
+                return ctl
+            chunk = min(2 * chunk, cap)
 
     def set_block_size(self, block: int) -> None:
         self._struct.block_size = int(block)
@@ -177,29 +199,42 @@ class BatchedEulerSolver:
                                                 ws.stage.data_ptr(), stream))
         _native.check(self._lib.cfd_run_control(C.byref(self._struct), stream))
 
+    def _persistent_chunk(self, attempts: int, stream) -> None:
+        ws = self._ws
+        _native.check(self._lib.cfd_batch_advance(C.byref(self._struct), ws.x0.data_ptr(), ws.x1.data_ptr(),
+                                                  ws.stage.data_ptr(), int(attempts), stream))
+
+    def _issue(self, n: int, stream) -> None:
+        if self.persistent:
+            self._persistent_chunk(n, stream)
+        else:
+            for _ in range(n):
+                self._attempt_and_control(stream)
+
     def _chunk_graph(self, n: int):
         import torch
 
-        g = self._graphs.get(n)
+        key = (n, self.persistent)
+        g = self._graphs.get(key)
         if g is None:
+            if self.persistent:  # the per-device lookup of the resident grid, outside the capture
+                self._persistent_chunk(0, torch.cuda.current_stream().cuda_stream)
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=side):
-                s = torch.cuda.current_stream().cuda_stream
-                for _ in range(n):
-                    self._attempt_and_control(s)
+                self._issue(n, torch.cuda.current_stream().cuda_stream)
             torch.cuda.current_stream().wait_stream(side)
-            self._graphs[n] = g
+            self._graphs[key] = g
         return g
 
     def advance(self, attempts: int, *, graph: bool = True) -> list:
+        """Run `attempts` attempt + control passes (no-ops for finished
+        instances) and return every instance's loop state."""
         if graph:
             self._chunk_graph(attempts).replay()
         else:
-            s = _stream()
-            for _ in range(attempts):
-                self._attempt_and_control(s)
+            self._issue(attempts, _stream())
         return self.controls()
 
     def run(self, states=None, final_time=None, *, graph: bool = True) -> list[RunResult]:

@@ -6,7 +6,8 @@ Steps: (1) print the degree-4 reference-triangle tables as compile-time
 constants into ``csrc/tables.cuh``; (2) compile the objects with nvcc for
 ``sm_100a`` in parallel — ``kernels.cu`` (limiter, adjoint, small kernels and
 the C ABI) and ``stage_inst.cu`` once per precision x mode of the fused stage
-kernels — into ``_build/``, each rebuilt only when its inputs change; (3) link
+kernels and ``batch_inst.cu`` once per precision x flux of the persistent
+batch kernel — into ``_build/``, each rebuilt only when its inputs change; (3) link
 them into ``cfd_demo_b200/libcfd_b200.so`` (in-tree, so it travels with the
 repository snapshot). No CUDA device is needed to build.
 """
@@ -33,9 +34,12 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
 ]
 # (object name, source, extra defines)
-OBJECTS = [("kernels", "kernels.cu", [])] + [
+OBJECTS = [("kernels", "kernels.cu", []), ("setup", "setup.cu", [])] + [
     (f"stage_{prec}_{mode}", "stage_inst.cu", [f"-DCFD_STAGE_PREC={p}", f"-DCFD_STAGE_MODE={m}"])
     for p, prec in enumerate(("f64", "f32")) for m, mode in enumerate(("rhs", "limited", "unlimited"))
+] + [
+    (f"batch_{prec}_{flux}", "batch_inst.cu", [f"-DCFD_BATCH_PREC={p}", f"-DCFD_BATCH_FLUX={f}"])
+    for p, prec in enumerate(("f64", "f32")) for f, flux in enumerate(("rusanov", "roe", "hllc"))
 ]
 
 

@@ -5,6 +5,7 @@
 // (stage_inst.cu, one per precision and mode) beside kernels.cu, which holds
 // the limiter, adjoint and small kernels and the C ABI.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -434,8 +435,15 @@ __device__ __forceinline__ R stage3_combine(R b, R v) {
 
 #include "stage_pair.cuh"
 #include "stage_tile.cuh"
+#include "limiter.cuh"
+#include "control.cuh"
+#include "batch.cuh"
 
 inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// Records `msg` as the calling thread's last error (cfd_last_error) and
+// returns `code`; defined in kernels.cu.
+int cfd_fail(int code, const char* msg);
 
 // ---------------------------------------------------- stage-kernel launches ---
 template <typename R, int FLUX, int MODE>
@@ -452,9 +460,9 @@ void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream_t st) 
   else launch_stage_bs<R, 2, MODE>(p, bs, st);
 }
 template <typename R, int FLUX, int MODE, int EPB, bool SB, int MINB = (sizeof(R) == 4 ? 512 : 384) / (2 * EPB),
-          bool UF = true, bool PK = true, bool CF = false>
+          bool UF = true, bool PK = true, bool CF = false, bool FJ = false>
 void launch_tile(const StageParams& p, cudaStream_t st) {
-  using L = TileLayout<R, EPB, SB>;
+  using L = TileLayout<R, EPB, SB, FJ>;
   constexpr bool PACK = PK && sizeof(R) == 4;  // FP64 shares the unpacked instantiation
   constexpr bool CALL = CF && sizeof(R) == 4;
   // opt in to > 48 KB of dynamic shared memory, once per instantiation and
@@ -465,12 +473,12 @@ void launch_tile(const StageParams& p, cudaStream_t st) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= MAX_DEV || !configured[dev]) {
-    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL>,
+    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL, FJ>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
     if (dev >= 0 && dev < MAX_DEV) configured[dev] = true;
   }
   const unsigned g = blocks_for(p.m.num_elements, EPB);
-  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL><<<g, 2 * EPB, L::BYTES, st>>>(p);
+  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL, FJ><<<g, 2 * EPB, L::BYTES, st>>>(p);
 }
 template <typename R, int FLUX, int MODE>
 void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_t st) {
@@ -484,6 +492,10 @@ void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_
   else if (variant == 7) launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, false, false>(p, st);
   else if (variant == 8) launch_tile<R, FLUX, MODE, 64, true>(p, st);
   else if (variant == 9) launch_tile<R, FLUX, MODE, 64, true, (sizeof(R) == 4 ? 512 : 384) / 128, true, true, true>(p, st);
+  // 10 / 11: the face-job form (each face's flux once for both sides), without / with staged base rows
+  else if (variant == 10)
+    launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, true, true, true, true>(p, st);
+  else if (variant == 11) launch_tile<R, FLUX, MODE, 64, true, sizeof(R) == 4 ? 3 : 2, true, true, true, true>(p, st);
   else launch_tile<R, FLUX, MODE, 32, false>(p, st);
 }
 // One precision and mode of the stage kernels, every flux and shape; each

@@ -21,272 +21,6 @@
 
 namespace cfd {
 
-// ----------------------------------------------------------- limit kernel ---
-struct LimitParams {
-  CfdMesh m;
-  const CfdControl* ctl;  // null: always active (cfd_limit)
-  const void* x0;
-  const void* x1;
-  void* stage;
-  int stage_idx;          // 1..3, or 0 with q = q_io (cfd_limit)
-  void* q_io;
-  double gamma;
-  const double* avg;
-  const double* aux;
-  CfdStageAcc* acc;       // stage mode
-  int32_t* troubled_out;  // cfd_limit mode
-  double* pos_out;        // optional [2][ld]: pressure-scaling theta and its critical node
-  int* list;              // two-pass form: elements for the rewrite pass, and
-  int* count;             // their number (zeroed before the scan)
-  uint8_t* flags;         // optional [ld]: troubled-cell indicator per element
-};
-
-// Cockburn-Shu troubled-cell limiter (limiting.py:136-163) followed by the
-// positivity limiter (limiting.py:166-200), in place on the stage state, for
-// element e of instance inst. PART 0: everything in one pass; PART 1 (scan):
-// elements the limiters leave as they are contribute their minima, the others
-// are only marked `listed`; PART 2: the rewrite of a listed element.
-template <typename R, int PHI, int PART>
-__device__ __forceinline__ void limit_body(const LimitParams& P, int e, int par, Red& red, bool& listed) {
-  const CfdMesh& m = P.m;
-  const int ld = m.ld;
-  {
-    R* __restrict__ q;
-    if (P.stage_idx == 0) {
-      q = (R*)P.q_io;
-    } else if (P.stage_idx == 2) {
-      q = (R*)P.stage;
-    } else {
-      q = (R*)(par ? P.x0 : P.x1);
-    }
-    const double gm1 = P.gamma - 1.0;
-    double a[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) a[c] = P.avg[c * ld + e];
-    const double pa = pressure_x(a[0], a[1], a[2], a[3], gm1);
-    const double eps = jmin(POSITIVITY_FLOOR, jmin(a[0], pa));
-    const double pt = pressure_target<R>(eps, pa, a[3], gm1);
-    const double det_tol = sizeof(R) == 8 ? DETECTION_TOLERANCE : DETECTION_TOLERANCE_FP32;
-    const int finfo = m.face_info[e];
-    bool troubled = false;
-    R scaled[3][4];
-    if (PHI != LIM_UNLIMITED) {
-      // neighbour / ghost averages (limiting.py:128-133), unfused as in NumPy
-      R diff[3][4];
-      const double* fgd = m.face_geo;
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        const int kind = (finfo >> (8 * f)) & 3;
-        double na[4];
-        if (kind == CFD_FACE_INTERIOR) {
-          const int nb = m.neighbor[f * ld + e];
-#pragma unroll
-          for (int c = 0; c < 4; ++c) na[c] = P.avg[c * ld + nb];
-        } else if (kind == CFD_FACE_SLIP_WALL) {
-          const double nx = fgd[(3 * f) * ld + e], ny = fgd[(3 * f + 1) * ld + e];
-          const double mn = xadd(xmul(a[1], nx), xmul(a[2], ny));
-          na[0] = a[0];
-          na[1] = xsub(a[1], xmul(xmul(2.0, mn), nx));
-          na[2] = xsub(a[2], xmul(xmul(2.0, mn), ny));
-          na[3] = a[3];
-        } else {
-          const int row = m.neighbor[f * ld + e];
-#pragma unroll
-          for (int c = 0; c < 4; ++c) na[c] = m.bc_states[row * 4 + c];
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) diff[f][c] = (R)xsub(na[c], a[c]);
-      }
-      const R* __restrict__ cs = GeoPtr<R>::cs(m);
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        const int pf = (finfo >> (8 * f + 4)) & 3;
-        const R al = cs[f * ld + e], be = cs[(3 + f) * ld + e];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const R pd = pf == 0 ? diff[0][c] : (pf == 1 ? diff[1][c] : diff[2][c]);
-          scaled[f][c] = xmul((R)NEIGHBOR_FACTOR, xadd(xmul(al, diff[f][c]), xmul(be, pd)));
-        }
-      }
-      // detection on rho and E at the three face midpoints (limiting.py:147-151)
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-          const int c = cc == 0 ? 0 : 3;
-          const R tr = xsub(q[(c * NP + tab::MID_NODES[f]) * ld + e], (R)a[c]);
-          const R ex = abs_(xsub(minmod2(tr, scaled[f][c]), tr));
-          troubled |= (double)ex > xmul(det_tol, fabs(a[c]));
-        }
-      }
-    }
-    if (PART != 2 && P.flags) P.flags[e] = troubled ? 1 : 0;
-    const double rmin0 = P.aux[e], pmin0 = P.aux[ld + e];
-    const bool need_pos = (rmin0 < eps) || (pmin0 < pt);
-    if (!troubled && !need_pos) {
-      red.kr = dkey(rmin0);
-      red.kp = dkey(pmin0);
-      if (P.stage_idx == 3) {
-        const double d = m.dt_geo[e] / P.aux[2 * ld + e];
-        red.kd = dkey(d);
-        if (d != d) red.fl |= FLAG_NAN_DT;
-      }
-    } else {
-      if (PART == 1) {  // the scan pass lists the element for the rewrite pass
-        listed = true;
-        return;
-      }
-      R s[NP][4];
-#pragma unroll
-      for (int i = 0; i < NP; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) s[i][c] = q[(c * NP + i) * ld + e];
-      if (troubled) {
-        // P1 midpoint values, phi-limited deltas, +/- rescaling, linear rebuild
-        // (limiting.py:153-162), in NumPy's operation order
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const R ac = (R)a[c];
-          R deltas[3];
-          R pos = R(0), neg = R(0);
-#pragma unroll
-          for (int f = 0; f < 3; ++f) {
-            R pr = xmul((R)tab::P1MID[f][0], s[0][c]);
-#pragma unroll
-            for (int i = 1; i < NP; ++i) pr = xadd(pr, xmul((R)tab::P1MID[f][i], s[i][c]));
-            pr = xsub(pr, ac);
-            R d = R(0);
-            if (pr != R(0)) d = xmul(pr, jmin(R(1), phi<R, PHI>(xdiv(scaled[f][c], pr))));
-            deltas[f] = d;
-            pos = f == 0 ? jmax(d, R(0)) : xadd(pos, jmax(d, R(0)));
-            neg = f == 0 ? jmax(-d, R(0)) : xadd(neg, jmax(-d, R(0)));
-          }
-          const R thp = pos > R(0) ? jmin(R(1), xdiv(neg, pos)) : R(0);
-          const R thn = neg > R(0) ? jmin(R(1), xdiv(pos, neg)) : R(0);
-#pragma unroll
-          for (int f = 0; f < 3; ++f)
-            deltas[f] = xsub(xmul(thp, jmax(deltas[f], R(0))), xmul(thn, jmax(-deltas[f], R(0))));
-#pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            R v = xmul((R)tab::LINBASIS[i][0], deltas[0]);
-            v = xadd(v, xmul((R)tab::LINBASIS[i][1], deltas[1]));
-            v = xadd(v, xmul((R)tab::LINBASIS[i][2], deltas[2]));
-            s[i][c] = xadd(ac, v);
-          }
-        }
-        red.tr = 1;
-      }
-      if (P.pos_out) {
-        double th;
-        int node;
-        positivity<R>(s, a, gm1, &th, &node);
-        P.pos_out[e] = th;
-        P.pos_out[ld + e] = (double)node;
-      } else {
-        positivity<R>(s, a, gm1);
-      }
-#pragma unroll
-      for (int i = 0; i < NP; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) q[(c * NP + i) * ld + e] = s[i][c];
-      double rmin, pmin, lam;
-      bool finite;
-      element_stats<R>(s, gm1, P.gamma, rmin, pmin, lam, finite);
-      if (!finite) red.fl |= FLAG_NONFINITE;
-      red.kr = dkey(rmin);
-      red.kp = dkey(pmin);
-      if (P.stage_idx == 3) {
-        const double d = m.dt_geo[e] / lam;
-        red.kd = dkey(d);
-        if (d != d) red.fl |= FLAG_NAN_DT;
-      }
-    }
-    }
-}
-
-template <typename R, int PHI, int BS>
-__global__ void __launch_bounds__(BS) limit_kernel(const LimitParams P) {
-  const CfdMesh& m = P.m;
-  const int e = blockIdx.x * BS + threadIdx.x;
-  bool live = e < m.num_elements;
-  int inst = 0;
-  if (live && m.instance) inst = m.instance[e];
-  if (inst < 0) {  // padding between instances
-    live = false;
-    inst = 0;
-  }
-  int par = 0;
-  if (live && P.ctl) {
-    live = P.ctl[inst].status == CFD_RUN_ACTIVE;
-    par = P.ctl[inst].parity;
-  }
-  Red red;
-  red.init();
-  bool listed = false;
-  if (live) limit_body<R, PHI, 0>(P, e, par, red, listed);
-  if (P.stage_idx == 0) {
-    if (live && red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
-  } else {
-    block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
-  }
-}
-
-// The same limiter in two passes. The scan runs the detection for every
-// element with few registers, commits the minima (and CFL step) of the
-// elements the limiters leave as they are, and lists the others (troubled,
-// or below the positivity floor: a small minority); the rewrite pass then
-// runs the full reconstruction and positivity scaling on the listed
-// elements only, committing their minima one element at a time. Same
-// arithmetic, same results as limit_kernel.
-template <typename R, int PHI, int BS>
-__global__ void __launch_bounds__(BS) limit_scan_kernel(const LimitParams P) {
-  const CfdMesh& m = P.m;
-  const int e = blockIdx.x * BS + threadIdx.x;
-  bool live = e < m.num_elements;
-  int inst = 0;
-  if (live && m.instance) inst = m.instance[e];
-  if (inst < 0) {
-    live = false;
-    inst = 0;
-  }
-  int par = 0;
-  if (live && P.ctl) {
-    live = P.ctl[inst].status == CFD_RUN_ACTIVE;
-    par = P.ctl[inst].parity;
-  }
-  Red red;
-  red.init();
-  bool listed = false;
-  if (live) limit_body<R, PHI, 1>(P, e, par, red, listed);
-  warp_list_append(P.list, P.count, listed, e);
-  if (listed) red.init();
-  if (P.stage_idx == 0) {
-    if (live && red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
-  } else {
-    block_commit<BS>(red, live && !listed, inst, P.acc, 3, P.stage_idx - 1);
-  }
-}
-
-template <typename R, int PHI>
-__global__ void __launch_bounds__(64) limit_rewrite_kernel(const LimitParams P) {
-  const CfdMesh& m = P.m;
-  const int n = *P.count;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int e = P.list[t];
-    const int inst = m.instance ? m.instance[e] : 0;
-    const int par = P.ctl ? P.ctl[inst].parity : 0;
-    Red red;
-    red.init();
-    bool listed = false;
-    limit_body<R, PHI, 2>(P, e, par, red, listed);
-    if (P.stage_idx == 0) {
-      if (red.tr) atomicAdd(&P.troubled_out[inst], red.tr);
-    } else {
-      commit_one(red, P.acc + 3 * inst + (P.stage_idx - 1));
-    }
-  }
-}
-
 // Averages + per-element minima of q_in, copied to q_out (cfd_limit prologue).
 template <typename R, int BS>
 __global__ void __launch_bounds__(BS) prep_kernel(CfdMesh m, const R* __restrict__ qin, R* __restrict__ qout,
@@ -350,91 +84,17 @@ __global__ void __launch_bounds__(BS) dt_kernel(CfdMesh m, const R* __restrict__
 __global__ void reset_acc_kernel(CfdStageAcc* acc, int n, int* list_counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 4 && list_counters) list_counters[i] = 0;  // the two-pass limiter's per-stage counters
-  if (i >= n) return;
-  CfdStageAcc z;
-  z.boundary_flux[0] = z.boundary_flux[1] = z.boundary_flux[2] = z.boundary_flux[3] = 0.0;
-  z.min_rho_key = z.min_p_key = z.dt_key = KEY_EMPTY;
-  z.troubled = 0;
-  z.flags = 0;
-  acc[i] = z;
+  if (i < n) reset_acc_one(acc, i);
 }
 
-__device__ __forceinline__ double key_min_value(unsigned long long k) {
-  return k == KEY_EMPTY ? INFINITY : dkey_decode(k);
-}
-
-// StepReport of one attempt (time_integration.py:69-83).
 __global__ void report_kernel(const CfdStageAcc* acc, const CfdControl* ctl, CfdStepReport* rep, int n, double cfl) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (ctl[i].status != CFD_RUN_ACTIVE) return;
-  const CfdStageAcc* a = acc + 3 * i;
-  const double dt = ctl[i].dt;
-  CfdStepReport r;
-  for (int c = 0; c < 4; ++c)
-    r.boundary_flux[c] = dt * (a[0].boundary_flux[c] / 6.0 + a[1].boundary_flux[c] / 6.0 + 2.0 * a[2].boundary_flux[c] / 3.0);
-  const int fl = a[0].flags | a[1].flags | a[2].flags;
-  r.admissible = (fl & FLAG_ADMISSIBILITY) == 0;
-  double rmin = INFINITY, pmin = INFINITY;
-  int tr = 0;
-  for (int s = 0; s < 3; ++s) {
-    rmin = fmin(rmin, key_min_value(a[s].min_rho_key));
-    pmin = fmin(pmin, key_min_value(a[s].min_p_key));
-    tr = max(tr, a[s].troubled);
-  }
-  if (fl & FLAG_NONFINITE) {
-    rmin = NAN;
-    pmin = NAN;
-  }
-  r.min_density = rmin;
-  r.min_pressure = pmin;
-  r.troubled_cells = tr;
-  r.dt = dt;
-  r.dt_next = (a[2].flags & FLAG_NAN_DT) ? (double)NAN : cfl * dkey_decode(a[2].dt_key);
-  r.reserved[0] = r.reserved[1] = 0;
-  rep[i] = r;
+  if (i < n) report_one(acc, ctl, rep, i, cfl);
 }
 
-// One pass of the body of solver.py:180-204 after an attempt.
 __global__ void run_control_kernel(CfdControl* ctl, const CfdStepReport* rep, int n, int max_rejections) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  CfdControl c = ctl[i];
-  if (c.status != CFD_RUN_ACTIVE) return;
-  const CfdStepReport r = rep[i];
-  if (r.admissible) {
-    c.parity ^= 1;
-    c.time = c.reaches_end ? c.final_time : c.time + c.dt;
-    c.steps += 1;
-    for (int k = 0; k < 4; ++k) c.flux_integral[k] += r.boundary_flux[k];
-    if (r.min_density < c.min_density) c.min_density = r.min_density;
-    if (r.min_pressure < c.min_pressure) c.min_pressure = r.min_pressure;
-    c.max_troubled = max(c.max_troubled, r.troubled_cells);
-    c.attempts = 0;
-    if (!(c.time < c.final_time)) {
-      c.status = CFD_RUN_DONE;
-    } else {
-      const double dt = r.dt_next;
-      if (!isfinite(dt) || dt <= 0.0) {
-        c.status = CFD_RUN_BAD_DT;
-        c.dt = dt;
-      } else {
-        const double remaining = c.final_time - c.time;
-        c.reaches_end = dt >= remaining;
-        c.dt = c.reaches_end ? remaining : dt;
-      }
-    }
-  } else {
-    c.rejected += 1;
-    c.attempts += 1;
-    if (c.attempts >= max_rejections + 1) {
-      c.status = CFD_RUN_REJECTED;
-    } else {
-      c.reaches_end = 0;
-      c.dt *= 0.5;
-    }
-  }
-  ctl[i] = c;
+  if (i < n) control_one(ctl, rep, i, max_rejections);
 }
 
 __global__ void run_init_kernel(CfdControl* ctl, const CfdStageAcc* acc, const double* final_time, int n, double cfl) {
@@ -566,6 +226,7 @@ static int fail(int code, const char* msg) {
   snprintf(g_err, sizeof(g_err), "%s", msg);
   return code;
 }
+int cfd::cfd_fail(int code, const char* msg) { return fail(code, msg); }
 static int check_launch(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -590,7 +251,7 @@ static int validate(const CfdSolver* s) {
   if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
   if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
     return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
-  if (s->variant < 0 || s->variant > 9) return fail(CFD_E_ARG, "variant must be 0..9");
+  if (s->variant < 0 || s->variant > 11) return fail(CFD_E_ARG, "variant must be 0..11");
   if (s->variant != 2 && s->mesh.instance && s->mesh.num_instances > 1 && (s->mesh.flags & 1) == 0)
     return fail(CFD_E_ARG, "tiled stage kernels need instance ranges aligned to 64 elements (CfdMesh.flags bit 0)");
   return CFD_OK;
@@ -889,6 +550,36 @@ int cfd_run_control(const CfdSolver* s, void* stream) {
   const int n = s->mesh.num_instances;
   run_control_kernel<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(s->control, s->report, n, s->max_rejections);
   return check_launch("cfd_run_control");
+}
+
+int cfd_batch_advance(const CfdSolver* s, void* x0, void* x1, void* stage, int32_t attempts, void* stream) {
+  int rc = attempt_args(s, x0, x1, stage);
+  if (rc) return rc;
+  if (!s->limit_list) return fail(CFD_E_ARG, "cfd_batch_advance: limit_list scratch is required");
+  if (attempts < 0) return fail(CFD_E_ARG, "cfd_batch_advance: attempts must be nonnegative");
+  BatchParams b;
+  memset(&b, 0, sizeof(b));
+  b.s = *s;
+  b.x0 = x0;
+  b.x1 = x1;
+  b.stage = stage;
+  b.attempts = attempts;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (s->precision == CFD_FP64) {
+    e = s->flux == 0 ? launch_batch_part<double, 0>(b, s->limiter, st)
+        : s->flux == 1 ? launch_batch_part<double, 1>(b, s->limiter, st)
+                       : launch_batch_part<double, 2>(b, s->limiter, st);
+  } else {
+    e = s->flux == 0 ? launch_batch_part<float, 0>(b, s->limiter, st)
+        : s->flux == 1 ? launch_batch_part<float, 1>(b, s->limiter, st)
+                       : launch_batch_part<float, 2>(b, s->limiter, st);
+  }
+  if (e != cudaSuccess) {
+    snprintf(g_err, sizeof(g_err), "cfd_batch_advance: %s", cudaGetErrorString(e));
+    return CFD_E_CUDA;
+  }
+  return check_launch("cfd_batch_advance");
 }
 
 int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, void* stream) {

@@ -243,6 +243,26 @@ __device__ __forceinline__ void trace_flux(const R qm[4], const R qp[4], R nx, R
   }
 }
 
+// The same, also returning the normal flux F(q+).n of the exterior trace
+// (with the interior normal): the face-job form lifts the neighbour's side
+// from it.
+template <typename R, int FLUX>
+__device__ __forceinline__ void trace_flux3(const R qm[4], const R qp[4], R nx, R ny, R gamma, R fhat[4], R fm[4],
+                                            R fp[4]) {
+  const R gm1 = gamma - R(1);
+  const Prim<R> wm = primitive(qm, gm1);
+  const Prim<R> wp = primitive(qp, gm1);
+  normal_flux(qm, wm, nx, ny, fm);
+  normal_flux(qp, wp, nx, ny, fp);
+  if (FLUX == FLUX_RUSANOV) rusanov(qm, qp, wm, wp, nx, ny, gamma, fm, fp, fhat);
+  else if (FLUX == FLUX_ROE) roe(qm, qp, wm, wp, nx, ny, gamma, fm, fp, fhat);
+  else hllc(qm, qp, wm, wp, nx, ny, gamma, fm, fp, fhat);
+  if (sizeof(R) == 4 && qm[0] == qp[0] && qm[1] == qp[1] && qm[2] == qp[2] && qm[3] == qp[3]) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) fhat[c] = fm[c];
+  }
+}
+
 enum { LIM_MINMOD = 0, LIM_MC = 1, LIM_VAN_LEER = 2, LIM_SUPERBEE = 3, LIM_UNLIMITED = 4 };
 
 // limiters.py:16-39

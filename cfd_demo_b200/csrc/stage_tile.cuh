@@ -30,8 +30,11 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// Shared-memory layout of one block (all offsets in elements of R, 16-byte aligned).
-template <typename R, int EPB, bool STAGE_BASE>
+// Shared-memory layout of one block (all offsets in elements of R, 16-byte
+// aligned). With FACE_JOBS the neighbour-trace region holds the traces of the
+// owned out-of-tile faces by face (TRC, [3 EPB][NFP][4]) and a jump region
+// (JMP, [EPB][3 NFP][4]) and the owned-face list follow.
+template <typename R, int EPB, bool STAGE_BASE, bool FACE_JOBS = false>
 struct TileLayout {
   // row stride of the [60][.] state tiles: 30 rows apart (the two lanes'
   // variables) must fall 16 banks apart, and rows must stay 16-byte aligned
@@ -43,10 +46,29 @@ struct TileLayout {
   // four 64-element FP32 blocks with base rows fit an SM's shared memory)
   static __device__ __forceinline__ int base_at(int row, int col) { return row * EPB + (row >= 30 ? 16 : 0) + col; }
   static constexpr int NBR = BASE + (STAGE_BASE ? 60 * EPB + 16 : 0);  // [8 rounds][4 vars][EPB][2 lanes]
-  static constexpr int GEO = NBR + 64 * EPB;                      // [13][S]: rx ry sx sy, (nx ny fs) x 3
+  static constexpr int JMP = NBR + (FACE_JOBS ? 3 * EPB * NFP * 4 : 64 * EPB);
+  static constexpr int GEO = JMP + (FACE_JOBS ? EPB * 3 * NFP * 4 : 0);  // [13][S]: rx ry sx sy, (nx ny fs) x 3
   static constexpr int INT_BYTES_OFF = (GEO + 13 * S) * (int)sizeof(R);  // int rows [4][EPB]
-  static constexpr int BYTES = INT_BYTES_OFF + 4 * EPB * 4;
+  static constexpr int FACES_BYTES_OFF = INT_BYTES_OFF + 4 * EPB * 4;    // owned faces [3 EPB] + count
+  static constexpr int BYTES = FACES_BYTES_OFF + (FACE_JOBS ? 3 * EPB * 4 + 16 : 0);
 };
+
+// FACE_JOBS: the owner of a face computes its flux once for both sides. The
+// block lists the faces it owns (every boundary or out-of-tile face of its
+// elements, and each in-tile interior face once, by its lower-numbered
+// element), deals their face nodes out to all threads as jobs, and writes the
+// lifted-jump inputs of both elements into the jump region; a face F-hat of
+// the neighbour's side is -F-hat with its own normal, so the neighbour's
+// input is fs_nb (F-hat - F(q+).n).
+template <typename R> struct NodeFlux3 { R fhat[4], fm[4], fp[4]; };
+template <typename R, int FLUX>
+__device__ __noinline__ NodeFlux3<R> trace_flux3_call(R m0, R m1, R m2, R m3, R p0, R p1, R p2, R p3, R nx, R ny,
+                                                      R gamma) {
+  const R qm[4] = {m0, m1, m2, m3}, qp[4] = {p0, p1, p2, p3};
+  NodeFlux3<R> o;
+  trace_flux3<R, FLUX>(qm, qp, nx, ny, gamma, o.fhat, o.fm, o.fp);
+  return o;
+}
 
 // y0 += a x0, y1 += a x1. With PACK in the FP32 form: one packed
 // fma.rn.f32x2 (sm_100), each lane rounded exactly like a scalar fmaf, so the
@@ -164,11 +186,14 @@ __device__ __noinline__ NodeFlux<R> trace_flux_call(R m0, R m1, R m2, R m3, R p0
 // the lane's two variables (no effect in FP64); every launched FP32 shape
 // packs except the scalar reference shapes. CALL_FLUX: the face-node flux
 // as a call instead of eight inlined copies (FP32 form).
-template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB, bool UNROLL_FACES = true,
-          bool PACK = false, bool CALL_FLUX = false>
-__global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StageParams P) {
+// The stage work of one tile (EPB consecutive elements) by one block of
+// 2 EPB threads: the body of stage_tile_kernel, and of the persistent batch
+// kernel, whose blocks loop over tiles.
+template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, bool UNROLL_FACES = true, bool PACK = false,
+          bool CALL_FLUX = false, bool FACE_JOBS = false>
+__device__ __forceinline__ void stage_tile_body(const StageParams& P, const int tile) {
   constexpr int BS = 2 * EPB;
-  using L = TileLayout<R, EPB, STAGE_BASE>;
+  using L = TileLayout<R, EPB, STAGE_BASE, FACE_JOBS>;
   constexpr int S = L::S;
   constexpr int VEC = 16 / (int)sizeof(R);  // elements per 16-byte chunk
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -177,6 +202,8 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
   R* t_nbr = reinterpret_cast<R*>(smem_raw) + L::NBR;
   R* t_geo = reinterpret_cast<R*>(smem_raw) + L::GEO;
   int* t_int = reinterpret_cast<int*>(smem_raw + L::INT_BYTES_OFF);
+  R* t_jmp = reinterpret_cast<R*>(smem_raw) + L::JMP;  // FACE_JOBS: [EPB][3 NFP][4]
+  int* t_faces = reinterpret_cast<int*>(smem_raw + L::FACES_BYTES_OFF);  // FACE_JOBS: owned faces, count last
   __shared__ R s_rep[BS / 32][4 * NP];  // one element per warp for the rare positivity repair
 
   const CfdMesh& m = P.m;
@@ -185,7 +212,7 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
   const int tid = threadIdx.x;
   const int half = tid & 1;
   const int slot = tid >> 1;
-  const int e0 = blockIdx.x * EPB;
+  const int e0 = tile * EPB;
   const int e = e0 + slot;
   // block-uniform instance and loop state
   const int inst_raw = m.instance ? m.instance[e0] : 0;
@@ -261,7 +288,57 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
     }
     // ---- group B: neighbour face traces (this lane's two variables) and the base rows
     const int finfo = t_int[slot];
-    if (live) {
+    int nfaces = 0;
+    if constexpr (FACE_JOBS) {
+      // the owned faces, in a fixed order: lanes of element slot s test faces
+      // {0, 1} (even lane) and {2} (odd lane); warp prefix sums give the slots
+      unsigned own = 0;
+      if (live) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int f = half ? 2 : q;
+          if (half && q == 1) break;
+          const int info = (finfo >> (8 * f)) & 0xff;
+          bool mine = true;
+          if ((info & 3) == CFD_FACE_INTERIOR) {
+            const int nb = t_int[(1 + f) * EPB + slot];
+            mine = nb - e0 < 0 || nb - e0 >= EPB || nb > e;
+          }
+          if (mine) own |= 1u << q;
+        }
+      }
+      const int cnt = __popc(own);
+      const int lane = tid & 31, warp = tid >> 5;
+      int pre = cnt;  // inclusive warp prefix
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, pre, o);
+        if (lane >= o) pre += v;
+      }
+      __shared__ int s_wsum[BS / 32];
+      if (lane == 31) s_wsum[warp] = pre;
+      __syncthreads();
+      int off = pre - cnt;
+      for (int w = 0; w < warp; ++w) off += s_wsum[w];
+      for (int q = 0; q < 2; ++q)
+        if ((own >> q) & 1u) t_faces[off++] = slot | ((half ? 2 : q) << 8);
+      nfaces = 0;
+      for (int w = 0; w < BS / 32; ++w) nfaces += s_wsum[w];
+      __syncthreads();
+      // traces of the owned out-of-tile faces: TRC[face][k][c]
+      for (int i = tid; i < nfaces * NFP * 4; i += BS) {
+        const int fi = i / (NFP * 4), kc = i - fi * (NFP * 4), k = kc >> 2, c = kc & 3;
+        const int fe = t_faces[fi], os = fe & 0xff, f = fe >> 8;
+        const int info = (t_int[os] >> (8 * f)) & 0xff;
+        if ((info & 3) != CFD_FACE_INTERIOR) continue;
+        const int nb = t_int[(1 + f) * EPB + os];
+        if (nb - e0 >= 0 && nb - e0 < EPB) continue;
+        const int nf = (info >> 2) & 3;
+        const bool same_order = (f == 2) != (nf == 2);
+        const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);
+        cp_async_small<sizeof(R)>(&t_nbr[i], src + (size_t)(c * NP + pn) * ld + nb);
+      }
+    } else if (live) {
 #pragma unroll
       for (int sl = 0; sl < 3 * NFP; ++sl) {
         const int f = sl / NFP, k = sl % NFP;
@@ -334,11 +411,84 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
     cp_async_wait<0>();
     __syncthreads();
 
+    if constexpr (FACE_JOBS) {
+      // ---- surface term (dg.py:153-164) by face-node jobs: each owned face's
+      // nodes once, writing the lifted-jump inputs of both sides
+      for (int j = tid; j < nfaces * NFP; j += BS) {
+        const int fi = j / NFP, k = j - fi * NFP;
+        const int fe = t_faces[fi], os = fe & 0xff, f = fe >> 8;
+        const int info = (t_int[os] >> (8 * f)) & 0xff;
+        const int kind = info & 3;
+        const R nx = t_geo[(4 + 3 * f) * S + os], ny = t_geo[(5 + 3 * f) * S + os];
+        const R fs = t_geo[(6 + 3 * f) * S + os];
+        const int n = face_node_rt(f, k);
+        R qm[4], qp[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) qm[c] = t_own[(c * NP + n) * S + os];
+        int ns = -1, nslot = 0;  // in-tile neighbour: its slot and jump slot
+        if (kind == CFD_FACE_INTERIOR) {
+          const int nb = t_int[(1 + f) * EPB + os];
+          const int nf = (info >> 2) & 3;
+          const bool same_order = (f == 2) != (nf == 2);
+          const int kk = same_order ? k : NFP - 1 - k;
+          if (nb - e0 >= 0 && nb - e0 < EPB) {
+            ns = nb - e0;
+            nslot = nf * NFP + kk;
+            const int pn = face_node_rt(nf, kk);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) qp[c] = t_own[(c * NP + pn) * S + ns];
+          } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) qp[c] = t_nbr[j * 4 + c];
+          }
+        } else if (kind == CFD_FACE_SLIP_WALL) {  // dg.py:119-126
+          const R mn = qm[1] * nx + qm[2] * ny;
+          qp[0] = qm[0];
+          qp[1] = qm[1] - R(2) * mn * nx;
+          qp[2] = qm[2] - R(2) * mn * ny;
+          qp[3] = qm[3];
+        } else {
+          const int row = t_int[(1 + f) * EPB + os];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
+        }
+        const NodeFlux3<R> o = trace_flux3_call<R, FLUX>(qm[0], qm[1], qm[2], qm[3], qp[0], qp[1], qp[2], qp[3], nx,
+                                                         ny, gamma);
+        R jm[4];
+        jump_pair<R, PACK>(fs, o.fm[0], o.fm[1], o.fhat[0], o.fhat[1], jm[0], jm[1]);
+        jump_pair<R, PACK>(fs, o.fm[2], o.fm[3], o.fhat[2], o.fhat[3], jm[2], jm[3]);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) t_jmp[(os * 3 * NFP + f * NFP + k) * 4 + c] = jm[c];
+        if (ns >= 0) {
+          const int nf = nslot / NFP;
+          const R fsn = t_geo[(6 + 3 * nf) * S + ns];
+          R jn[4];
+          jump_pair<R, PACK>(fsn, o.fhat[0], o.fhat[1], o.fp[0], o.fp[1], jn[0], jn[1]);
+          jump_pair<R, PACK>(fsn, o.fhat[2], o.fhat[3], o.fp[2], o.fp[3], jn[2], jn[3]);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) t_jmp[(ns * 3 * NFP + nslot) * 4 + c] = jn[c];
+        }
+        if (kind != CFD_FACE_INTERIOR) {
+          const double bw = ctab::FACE_W[k] * m.face_hlen[(size_t)f * ld + e0 + os];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) red.b[c] += bw * (double)o.fhat[c];
+        }
+      }
+      __syncthreads();
+      // ---- LIFT of the element's 15 jump inputs (this lane's two variables)
+#pragma unroll
+      for (int sl = 0; sl < 3 * NFP; ++sl) {
+        const R ja0 = t_jmp[(slot * 3 * NFP + sl) * 4 + c0], ja1 = t_jmp[(slot * 3 * NFP + sl) * 4 + c0 + 1];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) fma_pair<R, PACK>((R)tab::LIFT[i][sl], ja0, ja1, acc[i][0], acc[i][1]);
+      }
+    }
+
     // ---- surface term (dg.py:153-164): 8 rounds, the lanes take nodes 2r and 2r+1;
     // unrolled in the FP32 form so the LIFT columns are compile-time operands
     // (the FP64 form keeps the loop rolled: fewer live registers)
 #pragma unroll((sizeof(R) == 4 && UNROLL_FACES) ? 8 : 1)
-    for (int r = 0; r < 8; ++r) {
+    for (int r = 0; r < (FACE_JOBS ? 0 : 8); ++r) {
       const int sl = 2 * r + half;
       R jump[4] = {R(0), R(0), R(0), R(0)};
       if (sl < 3 * NFP) {
@@ -423,9 +573,14 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
 #include "stage_epilogue.inc"
     }
   }
-  if (!live) red.init();
+  if (!live) {  // a face-job thread may hold boundary-flux terms of live elements
+    double b[4] = {red.b[0], red.b[1], red.b[2], red.b[3]};
+    red.init();
+    if (FACE_JOBS && block_live)
+      for (int c = 0; c < 4; ++c) red.b[c] = b[c];
+  }
   if (MODE == MODE_RHS) {
-    if (live) {
+    if (live || FACE_JOBS) {
 #pragma unroll
       for (int c = 0; c < 4; ++c)
         if (red.b[c] != 0.0) atomicAdd(&P.bflux_out[inst * 4 + c], red.b[c]);
@@ -433,4 +588,10 @@ __global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StagePa
   } else {
     block_commit<BS>(red, live, inst, P.acc, 3, P.stage_idx - 1);
   }
+}
+
+template <typename R, int FLUX, int MODE, int EPB, bool STAGE_BASE, int MINB, bool UNROLL_FACES = true,
+          bool PACK = false, bool CALL_FLUX = false, bool FACE_JOBS = false>
+__global__ void __launch_bounds__(2 * EPB, MINB) stage_tile_kernel(const StageParams P) {
+  stage_tile_body<R, FLUX, MODE, EPB, STAGE_BASE, UNROLL_FACES, PACK, CALL_FLUX, FACE_JOBS>(P, blockIdx.x);
 }

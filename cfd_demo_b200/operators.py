@@ -229,9 +229,41 @@ def host_tables(mesh: TriangleMesh, connectivity: MeshConnectivity, geometry, re
     )
 
 
+def boundary_tag_tables(mesh: TriangleMesh, boundary_conditions) -> tuple[list, np.ndarray, np.ndarray, np.ndarray]:
+    """Per tag (sorted names, as mesh.py:150 orders them): boundary kind and
+    fixed-state row, and the distinct fixed exterior states (rows sorted as
+    np.unique sorts them, the host builder's bc_states). Raises the host
+    builder's errors for missing or unknown tags."""
+    tags = sorted(mesh.boundary_edges)
+    missing = sorted(set(tags) - set(boundary_conditions))
+    if missing:
+        raise ValueError(f"Boundary tags without a boundary condition: {missing}.")
+    unknown = sorted(set(boundary_conditions) - set(tags))
+    if unknown:
+        raise ValueError(f"Boundary conditions for tags that are not in the mesh: {unknown}.")
+    kinds = np.zeros(len(tags), dtype=np.int32)
+    fixed_states = []
+    for i, tag in enumerate(tags):
+        bc = boundary_conditions[tag]
+        if bc.kind not in (SLIP_WALL, FIXED_STATE):
+            raise ValueError(f"Unsupported boundary condition for tag {tag!r}: {bc!r}.")
+        kinds[i] = bc.kind
+        if bc.kind == FIXED_STATE and len(mesh.boundary_edges[tag]):
+            fixed_states.append(np.asarray(bc.state, dtype=np.float64))
+    rows = np.unique(np.stack(fixed_states), axis=0) if fixed_states else np.zeros((0, 4))
+    tag_row = np.zeros(len(tags), dtype=np.int32)
+    for i, tag in enumerate(tags):
+        bc = boundary_conditions[tag]
+        if bc.kind == FIXED_STATE and len(rows):
+            tag_row[i] = int(np.flatnonzero(np.all(rows == np.asarray(bc.state), axis=1))[0])
+    return tags, kinds, tag_row, rows
+
+
 class DeviceTables:
     """Mesh tables of one or more instances uploaded as torch tensors, plus the
-    ``CfdMesh`` struct pointing at them. Keeps the tensors alive."""
+    ``CfdMesh`` struct pointing at them. Keeps the tensors alive. Built from
+    host tables (several instances), or on the GPU from one mesh
+    (:meth:`build_on_device`)."""
 
     def __init__(self, parts: list[HostTables], device, precision: int):
         import torch
@@ -276,6 +308,10 @@ class DeviceTables:
         self.neighbor, self.face_info = t(nbr), t(info)
         self.instance = t(inst) if len(parts) > 1 else None
         self.bc_states = t(bcs)
+        self._finish(precision)
+
+    def _finish(self, precision: int) -> None:
+        """FP32 copies (mixed form) and the CfdMesh struct."""
         self.precision = precision
         if precision == _native.CFD_FP32_MIXED:
             self.metric32 = self.metric.float().contiguous()
@@ -285,6 +321,84 @@ class DeviceTables:
             self.metric32 = self.face_geo32 = self.cs_coef32 = None
         ptr = lambda x: None if x is None else x.data_ptr()  # noqa: E731
         self.struct = _native.CfdMesh(
-            k, ld, len(parts), 1 if len(parts) > 1 else 0, ptr(self.metric), ptr(self.face_geo), ptr(self.face_hlen), ptr(self.dt_geo),
-            ptr(self.jacobian), ptr(self.cs_coef), ptr(self.neighbor), ptr(self.face_info), ptr(self.instance),
-            ptr(self.bc_states), ptr(self.metric32), ptr(self.face_geo32), ptr(self.cs_coef32))
+            self.num_elements, self.ld, self.num_instances, 1 if self.num_instances > 1 else 0, ptr(self.metric),
+            ptr(self.face_geo), ptr(self.face_hlen), ptr(self.dt_geo), ptr(self.jacobian), ptr(self.cs_coef),
+            ptr(self.neighbor), ptr(self.face_info), ptr(self.instance), ptr(self.bc_states), ptr(self.metric32),
+            ptr(self.face_geo32), ptr(self.cs_coef32))
+
+    def with_precision(self, precision: int) -> "DeviceTables":
+        """The same FP64 tables (shared, not copied) for another arithmetic form."""
+        other = object.__new__(DeviceTables)
+        for name in ("device", "offsets", "sizes", "num_elements", "ld", "num_instances", "metric", "face_geo",
+                     "face_hlen", "dt_geo", "jacobian", "cs_coef", "neighbor", "face_info", "instance", "bc_states"):
+            setattr(other, name, getattr(self, name))
+        other._finish(precision)
+        return other
+
+    @classmethod
+    def build_on_device(cls, mesh: TriangleMesh, boundary_conditions, reference, device, precision: int,
+                        relative_tolerance: float = 1e-9) -> "DeviceTables":
+        """One mesh's tables built by the GPU (cfd_mesh_build): geometry,
+        connectivity and boundary tags, Cockburn-Shu coefficients and the
+        face-node pairing check, bit for bit the host builder's tables. An
+        invalid mesh is reported with the host builder's error."""
+        import ctypes as C
+
+        import torch
+
+        tags, kinds, tag_row, rows = boundary_tag_tables(mesh, boundary_conditions)
+        dev = torch.device(device)
+        k = mesh.num_elements
+        ld = padded_ld(k)
+        lib = _native.load()
+        verts = torch.as_tensor(np.ascontiguousarray(mesh.vertices)).to(dev)
+        elems = torch.as_tensor(np.ascontiguousarray(mesh.elements, dtype=np.int64)).to(dev)
+        edge_list = [np.asarray(mesh.boundary_edges[t], dtype=np.int64).reshape(-1, 2) for t in tags]
+        edges = np.concatenate(edge_list) if edge_list else np.zeros((0, 2), np.int64)
+        edge_tag = np.concatenate([np.full(len(e), i, np.int32) for i, e in enumerate(edge_list)]) if edge_list \
+            else np.zeros(0, np.int32)
+        t_edges = torch.as_tensor(np.ascontiguousarray(edges)).to(dev)
+        t_tag = torch.as_tensor(edge_tag).to(dev)
+        t_kind = torch.as_tensor(kinds).to(dev)
+        t_row = torch.as_tensor(tag_row).to(dev)
+        fn = np.asarray(reference.face_nodes)
+        r, sv = reference.r[fn], reference.s[fn]
+        bary = torch.as_tensor(np.ascontiguousarray(np.stack([-(r + sv) / 2, (1 + r) / 2, (1 + sv) / 2], axis=-1))).to(dev)
+
+        self = object.__new__(cls)
+        self.device = dev
+        self.offsets = np.array([0, k], dtype=np.int64)
+        self.sizes = np.array([k], dtype=np.int64)
+        self.num_elements, self.ld, self.num_instances = k, ld, 1
+        z = lambda *shape, dtype=torch.float64: torch.zeros(shape, dtype=dtype, device=dev)  # noqa: E731
+        self.metric, self.face_geo, self.face_hlen = z(4, ld), z(9, ld), z(3, ld)
+        self.dt_geo, self.jacobian, self.cs_coef = z(ld), z(ld), z(6, ld)
+        self.neighbor, self.face_info = z(3, ld, dtype=torch.int32), z(ld, dtype=torch.int32)
+        self.instance = None
+        self.bc_states = torch.as_tensor(rows if len(rows) else np.zeros((1, 4))).to(dev)
+        out = _native.CfdMesh(k, ld, 1, 0, self.metric.data_ptr(), self.face_geo.data_ptr(),
+                              self.face_hlen.data_ptr(), self.dt_geo.data_ptr(), self.jacobian.data_ptr(),
+                              self.cs_coef.data_ptr(), self.neighbor.data_ptr(), self.face_info.data_ptr(), None,
+                              self.bc_states.data_ptr(), None, None, None)
+        inp = _native.CfdMeshBuild(len(mesh.vertices), k, ld, len(edges), len(tags), 0, verts.data_ptr(),
+                                   elems.data_ptr(), t_edges.data_ptr() if len(edges) else None,
+                                   t_tag.data_ptr() if len(edges) else None, t_kind.data_ptr() if len(tags) else None,
+                                   t_row.data_ptr() if len(tags) else None)
+        nbytes = int(lib.cfd_mesh_build_work_bytes(k, len(edges)))
+        work = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _native.check(lib.cfd_mesh_build(C.byref(inp), C.byref(out), bary.data_ptr(), float(relative_tolerance),
+                                         work.data_ptr(), nbytes, status.data_ptr(), stream))
+        code = int(status.item())
+        if code:
+            # the host builders raise the same errors with their messages
+            from .mesh import build_connectivity
+
+            conn = build_connectivity(mesh)
+            geo = element_geometry(mesh)
+            neighbor_coefficients(conn, geo)
+            check_face_pairing(mesh, conn, reference, relative_tolerance, geometry=geo)
+            raise ValueError(f"The mesh tables could not be built (status {code}).")
+        self._finish(precision)
+        return self

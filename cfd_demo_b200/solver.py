@@ -30,7 +30,7 @@ from .euler import NUM_VARIABLES
 from .fluxes import FLUX_IDS, get_interface_flux
 from .limiters import LIMITER_IDS, get_limiter_function
 from .mesh import TriangleMesh, build_connectivity, element_geometry, node_coordinates
-from .operators import DeviceTables, LimiterOperators, host_tables, limiter_operators, resolve_boundary_conditions
+from .operators import DeviceTables, LimiterOperators, limiter_operators, resolve_boundary_conditions
 from .reference_element import DEGREE, build_reference_triangle
 
 DEFAULT_CFL = 0.5  # time_integration.py:18
@@ -139,15 +139,31 @@ class EulerSolver:
         self.config = config
         self.boundary_conditions = MappingProxyType(dict(boundary_conditions))
         self.reference = build_reference_triangle(DEGREE)
-        self.connectivity = build_connectivity(mesh)
-        self.geometry = element_geometry(mesh)
-        kind, state = resolve_boundary_conditions(self.connectivity, self.boundary_conditions)
-        self._host = host_tables(mesh, self.connectivity, self.geometry, self.reference, kind, state, device=device)
+        # the kernels' mesh tables are built by the GPU (cfd_mesh_build); the
+        # host connectivity and geometry are computed when first asked for
+        self._tables = DeviceTables.build_on_device(mesh, self.boundary_conditions, self.reference, device,
+                                                    _native.CFD_FP64)
         self._finish_init(device, block_size, graph_chunk, variant)
+
+    @property
+    def connectivity(self):
+        """Face connectivity (mesh.py:115-185 of CFD-demo), built on the host on first use."""
+        conn = getattr(self, "_connectivity", None)
+        if conn is None:
+            conn = self._connectivity = build_connectivity(self.mesh)
+        return conn
+
+    @property
+    def geometry(self):
+        """Element geometry (mesh.py:188-243 of CFD-demo), computed on the host on first use."""
+        geo = getattr(self, "_geometry", None)
+        if geo is None:
+            geo = self._geometry = element_geometry(self.mesh)
+        return geo
 
     def _finish_init(self, device, block_size: int, graph_chunk: int, variant: int = 0) -> None:
         self.precision = PRECISIONS[self.config.precision]
-        self.operators = DeviceTables([self._host], device, self.precision)
+        self.operators = self._tables.with_precision(self.precision)
         self._lib = _native.load()
         self._ws = Workspace(self.operators, self.precision, self.config.limiter != "unlimited")
         self._graph_chunk = int(graph_chunk)
@@ -162,8 +178,11 @@ class EulerSolver:
         import dataclasses
 
         other = object.__new__(EulerSolver)
-        for name in ("mesh", "boundary_conditions", "reference", "connectivity", "geometry", "_host"):
+        for name in ("mesh", "boundary_conditions", "reference", "_tables"):
             setattr(other, name, getattr(self, name))
+        for name in ("_connectivity", "_geometry"):
+            if hasattr(self, name):
+                setattr(other, name, getattr(self, name))
         other.config = dataclasses.replace(self.config, precision=precision, **config_changes)
         other._finish_init(self.operators.device, self._struct.block_size, self._graph_chunk, self._struct.variant)
         return other

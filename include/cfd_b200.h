@@ -26,6 +26,8 @@
  *   cfd_check_state    src/cfd_demo/solver.py:170-176      initial admissibility
  *   cfd_interface_flux src/cfd_demo/fluxes.py:28-159       rusanov / roe / hllc
  *   cfd_limiter_phi    src/cfd_demo/limiters.py:16-57      phi(r)
+ *   cfd_mesh_build     src/cfd_demo/mesh.py:135-291, limiting.py:51-94  connectivity,
+ *                      geometry, Cockburn-Shu coefficients, face-node pairing
  */
 #ifndef CFD_B200_H
 #define CFD_B200_H
@@ -112,6 +114,35 @@ typedef struct CfdMesh {
     const float* cs_coef32;
 } CfdMesh;
 
+/*
+ * Input of cfd_mesh_build (device arrays): one mesh and its boundary tags.
+ * The tag tables give, per tag index, the boundary kind and, for fixed-state
+ * tags, the row of bc_states holding the exterior state.
+ */
+typedef struct CfdMeshBuild {
+    int32_t num_vertices;
+    int32_t num_elements;          /* K */
+    int32_t ld;                    /* leading dimension of the output tables, >= K */
+    int32_t num_boundary_edges;
+    int32_t num_tags;
+    int32_t reserved;
+    const double* vertices;        /* [Nv][2] */
+    const int64_t* elements;       /* [K][3] counterclockwise vertex ids, each < num_vertices */
+    const int64_t* boundary_edges; /* [nb][2] vertex ids of every tagged boundary edge */
+    const int32_t* boundary_tag;   /* [nb] tag index of each edge */
+    const int32_t* tag_kind;       /* [tags] CFD_FACE_SLIP_WALL | CFD_FACE_FIXED_STATE */
+    const int32_t* tag_row;        /* [tags] bc_states row of a fixed-state tag */
+} CfdMeshBuild;
+
+/* status bits of cfd_mesh_build */
+#define CFD_SETUP_NONCONFORMING 1         /* a face shared by more than two elements */
+#define CFD_SETUP_DOUBLE_TAG 2            /* a boundary edge with more than one tag */
+#define CFD_SETUP_UNTAGGED 4              /* a boundary face without a tag */
+#define CFD_SETUP_TAG_NOT_BOUNDARY 8      /* a tagged edge that is not a boundary face */
+#define CFD_SETUP_NO_COEFFICIENTS 16      /* no nonnegative Cockburn-Shu coefficients */
+#define CFD_SETUP_NOT_CONFORMING_NODES 32 /* neighbouring face nodes do not coincide */
+#define CFD_SETUP_TABLE_FULL 64           /* internal hash table full (not expected) */
+
 /* Per instance and per RK stage reduction slots (zeroed by cfd_rk3_attempt). */
 typedef struct CfdStageAcc {
     double boundary_flux[4];        /* sum of w * sJ * Fhat over boundary face nodes */
@@ -176,7 +207,9 @@ typedef struct CfdSolver {
                               contractions, which the other tiled shapes issue as packed
                               FP32x2 FMAs (bitwise the same results; FP64 runs 3 / 5),
                               8 tiled with 64 elements per block + staged base rows,
-                              9 as 8 with the face-node flux as an out-of-line call (FP32) */
+                              9 as 8 with the face-node flux as an out-of-line call (FP32),
+                              10 / 11 the face-job form of 3 / 8: each face's flux is evaluated
+                              once, by the block's owner of the face, for both of its sides */
     int32_t* limit_list;   /* optional [CFD_LIMIT_LIST_HEADER + ld] scratch: with it the limiter
                               runs in two passes (a light detection pass over every element,
                               then the rewrite of the troubled / non-positive ones only);
@@ -246,6 +279,24 @@ int cfd_rk3_finish(const CfdSolver* s, void* stream);
  */
 int cfd_run_control(const CfdSolver* s, void* stream);
 
+/*
+ * cfd_batch_advance: `attempts` passes of (cfd_rk3_attempt + cfd_run_control)
+ * for every instance in ONE persistent, cooperative launch (no counterpart in
+ * the reference, which solves one problem per EulerSolver; this is the
+ * batched form of its run loop, solver.py:180-204). The grid holds as many
+ * blocks as are resident on the GPU at once; they loop over the element
+ * tiles of all instances, with a grid-wide barrier between the phases of an
+ * attempt (zero the reduction slots; stage k and its limiter passes for
+ * k = 1, 2, 3; report and control). Returns early once no instance is active.
+ * Needs the limit_list scratch (the limiter runs in its two-pass form). The
+ * tile shape is fixed per precision (FP32: variant 9, FP64: variant 3) and the
+ * per-element arithmetic is that of the separate launches, so the results
+ * equal those of `attempts` x (cfd_rk3_attempt + cfd_run_control) bit for bit.
+ * The first call on a device looks up the resident grid size: make it before
+ * any stream capture (a call with attempts = 0 does only that).
+ */
+int cfd_batch_advance(const CfdSolver* s, void* x0, void* x1, void* stage, int32_t attempts, void* stream);
+
 /* cfd_run_init: control[i] = {time 0, final_time[i], dt = clipped CFL step of
  * the current state, ...}; minima start from the nodal minima of the state. */
 int cfd_run_init(const CfdSolver* s, const void* x0, const double* final_time, void* stream);
@@ -313,6 +364,24 @@ int cfd_rk3_step_fixed(const CfdSolver* s, const void* q_in, void* q_out, void* 
                        void* stream);
 int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape, const double* dt, const void* g_out,
                          void* g_in, double* bc_bar, int32_t flags, void* work, void* stream);
+
+/*
+ * ---- mesh tables on the GPU
+ * cfd_mesh_build: the mesh tables of `out` (metric, face_geo, face_hlen,
+ * dt_geo, jacobian, cs_coef, neighbor, face_info; out->ld == in->ld and
+ * out->num_elements == in->num_elements; the pointers must be writable device
+ * memory) from the vertex and element arrays: geometry (mesh.py:216-243),
+ * face connectivity and boundary tags (mesh.py:135-185), Cockburn-Shu
+ * coefficients (limiting.py:51-94), every floating-point value bit for bit
+ * the host builder's. face_node_bary: [3][5][3] barycentric weights of the
+ * reference face nodes, for the check that face node k of face f meets node
+ * k or 4 - k of the neighbour's face (mesh.py:254-291) within pairing_rtol of
+ * the edge length. `work` is scratch of cfd_mesh_build_work_bytes bytes;
+ * *status (device) receives CFD_SETUP_* bits describing an invalid input.
+ */
+int64_t cfd_mesh_build_work_bytes(int32_t num_elements, int32_t num_boundary_edges);
+int cfd_mesh_build(const CfdMeshBuild* in, const CfdMesh* out, const double* face_node_bary, double pairing_rtol,
+                   void* work, int64_t work_bytes, int32_t* status, void* stream);
 
 /* ---- pointwise physics (exercise the device functions of the fused kernels) */
 int cfd_interface_flux(int32_t flux, int32_t n, const double* q_minus, const double* q_plus,

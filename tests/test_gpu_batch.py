@@ -9,14 +9,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("fp64", 2), ("fp32_mixed", 0), ("fp32_mixed", 3)])
-def test_batch_matches_single_instance_runs(precision, variant):
+@pytest.mark.parametrize("precision,variant,persistent", [("fp64", 0, False), ("fp64", 2, False),
+                                                          ("fp32_mixed", 0, False), ("fp32_mixed", 3, False),
+                                                          ("fp64", 3, True), ("fp32_mixed", 9, True)])
+def test_batch_matches_single_instance_runs(precision, variant, persistent):
     from cfd_demo_b200 import EulerSolver, SolverConfig
     from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
 
     cases = riemann_batch(count=6, seed=3, nx_range=(10, 40))
     cfg = SolverConfig(flux="hllc", limiter="superbee", gamma=1.4, precision=precision)
-    batch = BatchedEulerSolver(cases, cfg, variant=variant)
+    batch = BatchedEulerSolver(cases, cfg, variant=variant, persistent=persistent)
     results = batch.run(final_time=0.02)
     tol = 1e-12 if precision == "fp64" else 1e-6
     for case, res in zip(cases, results):
@@ -30,15 +32,43 @@ def test_batch_matches_single_instance_runs(precision, variant):
         np.testing.assert_allclose(res.boundary_flux_integral, ref.boundary_flux_integral, rtol=1e-9, atol=1e-12)
 
 
-def test_batch_instances_finish_at_their_own_times():
+@pytest.mark.parametrize("persistent", [True, False])
+def test_batch_instances_finish_at_their_own_times(persistent):
     from cfd_demo_b200 import SolverConfig
     from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
 
     cases = riemann_batch(count=5, seed=1, nx_range=(8, 24))
-    batch = BatchedEulerSolver(cases, SolverConfig(flux="rusanov", limiter="minmod", gamma=1.4))
+    batch = BatchedEulerSolver(cases, SolverConfig(flux="rusanov", limiter="minmod", gamma=1.4), persistent=persistent)
     times = np.array([0.005, 0.01, 0.0, 0.02, 0.015])
     res = batch.run(final_time=times)
     assert [r.time for r in res] == pytest.approx(list(times), abs=0.0)
     assert res[2].steps == 0
     for r, case in zip(res, cases):
         assert np.all(np.isfinite(r.state))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
+@pytest.mark.parametrize("flux,limiter", [("rusanov", "minmod"), ("roe", "unlimited"), ("hllc", "van_leer"),
+                                          ("hllc", "superbee"), ("rusanov", "mc")])
+def test_persistent_launch_is_bitwise_the_separate_launches(precision, flux, limiter):
+    """cfd_batch_advance (one cooperative launch per chunk, grid-wide barriers
+    between the phases) against graph chunks of cfd_rk3_attempt +
+    cfd_run_control with the same tile shape: identical bits, steps, times
+    and loop states, with and without CUDA-graph capture of the persistent
+    launch, in chunks that end in the middle of the run."""
+    from cfd_demo_b200 import SolverConfig
+    from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
+
+    cases = riemann_batch(count=7, seed=11, nx_range=(6, 30))
+    cfg = SolverConfig(flux=flux, limiter=limiter, gamma=1.4, precision=precision)
+    shape = 9 if precision == "fp32_mixed" else 3
+    ref = BatchedEulerSolver(cases, cfg, variant=shape, persistent=False).run(final_time=0.012)
+    for graph in (True, False):
+        batch = BatchedEulerSolver(cases, cfg, variant=shape, persistent=True, graph_chunk=5)
+        out = batch.run(final_time=0.012, graph=graph)
+        for a, b in zip(out, ref):
+            assert (a.steps, a.rejected_steps, a.max_troubled_cells) == (b.steps, b.rejected_steps, b.max_troubled_cells)
+            assert a.time == b.time and a.min_density == b.min_density and a.min_pressure == b.min_pressure
+            assert np.array_equal(a.state, b.state), np.abs(a.state - b.state).max()
+            # the boundary-flux integral sums floating-point atomics: order-dependent last bits
+            np.testing.assert_allclose(a.boundary_flux_integral, b.boundary_flux_integral, rtol=1e-12, atol=1e-15)
