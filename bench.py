@@ -562,7 +562,8 @@ def run_adjoint(args) -> dict:
     g = runner.pack(torch.stack([case.weight] + [torch.zeros_like(case.weight)] * 3, dim=-1))
 
     def timed(fn, repeats=3):
-        fn()  # warm-up
+        fn()  # warm-up (eager)
+        fn()  # warm-up (captures the CUDA graphs)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         start.record()
