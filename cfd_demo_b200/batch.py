@@ -128,15 +128,17 @@ class BatchedEulerSolver:
         self._struct.variant = int(variant)
         self._graphs.clear()
 
-    def run_to(self, states, final_time, *, max_chunk: int | None = None) -> list:
+    def run_to(self, states, final_time, *, max_chunk: int | None = None, max_attempts: int | None = None) -> list:
         """Advance every instance from t = 0 until each has ended (done, or
-        stopped by a bad CFL step or too many rejections, without raising);
-        returns the loop states (CfdControl) of all instances."""
+        stopped by a bad CFL step or too many rejections, without raising),
+        or `max_attempts` attempts have run (instances still active are left
+        so); returns the loop states (CfdControl) of all instances."""
         self.begin_run(states, final_time)
-        chunk, cap = 1, max_chunk or self._graph_chunk
+        chunk, cap, done = 1, max_chunk or self._graph_chunk, 0
         while True:
             ctl = self.advance(chunk)
-            if all(c.status != _native.RUN_ACTIVE for c in ctl):
+            done += chunk
+            if all(c.status != _native.RUN_ACTIVE for c in ctl) or (max_attempts and done >= max_attempts):
                 return ctl
             chunk = min(2 * chunk, cap)
 

@@ -9,7 +9,8 @@
 // Finished instances are skipped by the bodies; the loop ends early once no
 // instance is active. The per-tile and per-element work is exactly the
 // stage / limiter / control code of the separate launches, so the results are
-// theirs bit for bit.
+// theirs: bit for bit in FP32-mixed, to an ulp in FP64 (the compiler may
+// contract a multiply-add of the plain form differently in the two kernels).
 // Included by common.cuh inside namespace cfd.
 #pragma once
 

