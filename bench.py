@@ -235,7 +235,7 @@ def _barrier(world: int) -> None:
 
 
 def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: bool = True, sampler=None,
-                min_seconds: float = 1.0, max_repeats: int = 200) -> dict:
+                min_seconds: float = 1.0, max_repeats: int = 200, repeats: int | None = None) -> dict:
     """Advance the resident state `warmup` + `steps` RK3 steps (device CFL dt,
     device run-loop control); time the `steps` with CUDA events on the
     launching stream, and each stage launch separately. The block of exactly
@@ -286,8 +286,9 @@ def timed_steps(solver, steps: int, warmup: int, world: int = 1, stage_events: b
     t, sm = block()
     totals.append(t)
     stages.append(sm)
-    repeats = min(max_repeats, max(1, math.ceil(min_seconds * 1e3 / max(t, 1e-3))))
-    repeats = int(max_over_ranks([repeats], world, torch.device("cuda", torch.cuda.current_device()))[0])
+    if repeats is None:
+        repeats = min(max_repeats, max(1, math.ceil(min_seconds * 1e3 / max(t, 1e-3))))
+        repeats = int(max_over_ranks([repeats], world, torch.device("cuda", torch.cuda.current_device()))[0])
     for _ in range(repeats - 1):
         t, sm = block()
         totals.append(t)
@@ -347,7 +348,12 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     dof = k * NP_NODES
 
     results = {}
-    for name, solver in (("fp64", fp64), ("fp32_mixed", fp32)):
+    # FP32-mixed first: its block count is reused for FP64, so that both forms
+    # take the same number of steps and their end states can be compared
+    forms = (("fp32_mixed", fp32), ("fp64", fp64))
+    if args.profile_form:  # one form's timed steps only: the command line of the profiler captures
+        forms = tuple(f for f in forms if f[0] == args.profile_form)
+    for name, solver in forms:
         solver.begin_run(q0, math.inf)
         if name == "fp32_mixed":
             props = torch.cuda.get_device_properties(dev)
@@ -360,11 +366,20 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                 r = timed_steps(solver, steps, warmup, world, sampler=sampler)
             r["clocks"] = sampler.summary()
         else:
-            r = timed_steps(solver, steps, warmup, world)
+            r = timed_steps(solver, steps, warmup, world, repeats=results["fp32_mixed"]["repeats"]
+                            if "fp32_mixed" in results else None)
         r["state"] = solver.download(solver.state_tensor())
         # conservation defect over the whole run: final - initial integral + boundary flux
         r["defect"] = solver.integrate(r["state"]) - solver.integrate(q0) + r["flux_integral"]
         results[name] = r
+
+    if args.profile_form:
+        r = results[args.profile_form]
+        if rank == 0:
+            print(json.dumps({"profile_form": args.profile_form, "elements": fp32.mesh.num_elements,
+                              "ms_per_step": r["total_ms"] / steps, "stage_ms": [v / steps for v in r["stage_ms"]],
+                              "stage_kernel": list(tuned[args.profile_form]["choice"])}), flush=True)
+        return None
 
     # max over ranks of the timed region
     m32, m64 = max_over_ranks([results["fp32_mixed"]["total_ms"], results["fp64"]["total_ms"]], world, dev)
@@ -461,7 +476,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     return line
 
 
-def run_batch(args, sequential_stride: int = 1) -> dict:
+def run_batch(args, sequential_stride: int = 1, count: int | None = None) -> dict:
     """The batching form: seeded Riemann instances of uneven size (hllc/superbee,
     FP32-mixed) advanced together from t = 0 to t = 0.15, each with its own
     CFL steps, against the same instances advanced one at a time
@@ -477,7 +492,7 @@ def run_batch(args, sequential_stride: int = 1) -> dict:
     from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
 
     torch.cuda.set_device(0)
-    cases = riemann_batch(args.batch_count, seed=0)
+    cases = riemann_batch(count or args.batch_count, seed=0)
     cfg = SolverConfig(flux="hllc", limiter="superbee", gamma=1.4, precision="fp32_mixed")
     t_end = args.batch_final_time
     states = [c.initial_state for c in cases]
@@ -703,10 +718,12 @@ def main() -> None:
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing of the default line")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances timing of the default line")
+    ap.add_argument("--profile-form", choices=["fp32_mixed", "fp64"], default=None,
+                    help="time only this form's steps and print a short line (for profiler captures)")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-final-time", type=float, default=0.15)
     ap.add_argument("--batch-chunk", type=int, default=64, help="attempts per graph chunk of the batch run")
-    ap.add_argument("--batch-max-attempts", type=int, default=12000,
+    ap.add_argument("--batch-max-attempts", type=int, default=15000,
                     help="attempts after which instances still running are reported as such")
     ap.add_argument("--batch-stride", type=int, default=1, help="time every n-th instance in the sequential arm")
     args = ap.parse_args()
@@ -754,12 +771,13 @@ def main() -> None:
 
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
-    if rank == 0:
+    if rank == 0 and line is not None:
         line["cpu_baseline"] = base
         if world == 1 and not args.no_adjoint:
             line["adjoint"] = run_adjoint(args)
         if world == 1 and not args.no_batch:
-            line["batch"] = run_batch(args, sequential_stride=8)
+            # the first 64 instances of the family (the full 256: --workload batch)
+            line["batch"] = run_batch(args, sequential_stride=4, count=64)
         print(json.dumps(line), flush=True)
 
 

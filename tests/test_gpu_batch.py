@@ -57,7 +57,7 @@ def test_persistent_launch_is_bitwise_the_separate_launches(precision, flux, lim
     capture of the persistent launch, in chunks that end in the middle of the
     run: identical steps, rejections, troubled maxima and end times; FP32-mixed
     states and minima bit for bit (its contractions and combines are explicit
-    packed FMAs); FP64 to 1e-13 relative (the compiler may contract a
+    packed FMAs); FP64 to 1e-12 relative (the compiler may contract a
     multiply-add of the plain form into an FMA in one kernel and not in the
     other)."""
     from cfd_demo_b200 import SolverConfig
@@ -80,6 +80,47 @@ def test_persistent_launch_is_bitwise_the_separate_launches(precision, flux, lim
                 assert a.min_density == pytest.approx(b.min_density, rel=1e-13)
                 assert a.min_pressure == pytest.approx(b.min_pressure, rel=1e-12, abs=1e-18)
                 scale = np.maximum(np.abs(b.state).reshape(-1, 4).max(axis=0), 1e-300)
-                assert float((np.abs(a.state - b.state) / scale).max()) <= 1e-13
+                assert float((np.abs(a.state - b.state) / scale).max()) <= 1e-12
             # the boundary-flux integral sums floating-point atomics: order-dependent last bits
             np.testing.assert_allclose(a.boundary_flux_integral, b.boundary_flux_integral, rtol=1e-12, atol=1e-15)
+
+
+def test_near_vacuum_stall_is_the_reference_algorithms(report):
+    """Instance 25 of the seeded Riemann family (nx = 64; rho, p = 0.114,
+    0.561 | 0.782, 0.936; hllc/superbee) develops a near-vacuum at t ~ 0.0027
+    under the reference's algorithm: its CFL step falls by two orders of
+    magnitude within 80 steps and keeps falling, so the instance never
+    reaches t = 0.15 in any number of steps the benchmark allows. The FP64
+    GPU run follows the oracle's step sizes through the collapse."""
+    import oracle
+    from oracle.physics import FixedState as OFixed, SlipWall as OWall
+
+    from cfd_demo_b200 import EulerSolver, SolverConfig, _native
+    from cfd_demo_b200.batch import riemann_batch
+
+    case = riemann_batch(256, seed=0)[25]
+    m = case.mesh
+    om = oracle.mesh.TriangleMesh(np.array(m.vertices), np.array(m.elements),
+                                  {k: np.array(v) for k, v in m.boundary_edges.items()})
+    obcs = {t: (OFixed(tuple(b.state)) if b.kind == 2 else OWall()) for t, b in case.boundary_conditions.items()}
+    osolver = oracle.OracleSolver(om, obcs, flux="hllc", limiter="superbee", gamma=1.4)
+    steps = 100
+    q, odts = case.initial_state, []
+    for _ in range(steps):
+        dt = osolver.time_step(q)
+        q, rep = osolver.step(q, dt)
+        assert rep.admissible
+        odts.append(dt)
+    solver = EulerSolver(m, case.boundary_conditions, SolverConfig(flux="hllc", limiter="superbee", gamma=1.4))
+    solver.begin_run(case.initial_state, 0.15)
+    gdts = []
+    for _ in range(steps):
+        gdts.append(solver._read(solver._ws.control, _native.CfdControl).dt)
+        c = solver.advance(1)
+        assert c.status == _native.RUN_ACTIVE
+    odts, gdts = np.array(odts), np.array(gdts)
+    rel = float(np.max(np.abs(gdts - odts) / odts))
+    report(f"batch instance 25 (nx=64, hllc/superbee): oracle CFL step {odts[0]:.3g} -> {odts[-1]:.3g} in {steps} "
+           f"steps (t = {odts.sum():.5f}); GPU FP64 step sizes within {rel:.1e} of the oracle's")
+    assert odts[-1] < odts[0] / 50 and gdts[-1] < gdts[0] / 50
+    assert rel < 1e-2  # a borderline limiter decision may go the other way near the vacuum
