@@ -48,6 +48,7 @@ METRIC = "DOF-steps/s FP32-mixed vs FP64 plain at L1(rho)<=1e-5; adjoint/forward
 from cfd_demo_b200.workloads import JITTER, NX  # noqa: E402
 
 NP_NODES = 15
+PRECISION_STEPS = 25  # steps of the FP32-mixed vs FP64 comparison
 FALLBACK_HBM_GBS = 6650.0
 # Algorithmic bytes per element per RK3 step of the three stage launches:
 # state read + write per stage, the stage base state in stages 2-3, and the
@@ -363,14 +364,11 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                                       int(getattr(props, "pci_device_id", 0) or 0))
             sampler = ClockSampler(bus)
             with sampler:
-                r = timed_steps(solver, steps, warmup, world, sampler=sampler)
+                r = timed_steps(solver, steps, warmup, world, sampler=sampler, min_seconds=args.min_seconds)
             r["clocks"] = sampler.summary()
         else:
-            r = timed_steps(solver, steps, warmup, world, repeats=results["fp32_mixed"]["repeats"]
-                            if "fp32_mixed" in results else None)
-        r["state"] = solver.download(solver.state_tensor())
-        # conservation defect over the whole run: final - initial integral + boundary flux
-        r["defect"] = solver.integrate(r["state"]) - solver.integrate(q0) + r["flux_integral"]
+            r = timed_steps(solver, steps, warmup, world, min_seconds=args.min_seconds,
+                            repeats=results["fp32_mixed"]["repeats"] if "fp32_mixed" in results else None)
         results[name] = r
 
     if args.profile_form:
@@ -419,10 +417,18 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                                          f"{round(sum(sb) * k / 3)}",
                          "peak_source": peak_kind, "algorithmic_bytes_per_element_step": sum(sb)},
         }
-    l1 = l1_density(fp32, results["fp32_mixed"]["state"], results["fp64"]["state"])
-    linf = float(np.abs(results["fp32_mixed"]["state"][..., 0] - results["fp64"]["state"][..., 0]).max())
-    conservation = {n: {"mass_defect": float(results[n]["defect"][0]), "energy_defect": float(results[n]["defect"][3]),
-                        "time": results[n]["time"], "steps": results[n]["steps_done"]} for n in ("fp32_mixed", "fp64")}
+    # precision: both forms advance the same state by PRECISION_STEPS steps of
+    # the run loop (each with its own device CFL steps), untimed
+    states, conservation = {}, {}
+    for name, solver in (("fp32_mixed", fp32), ("fp64", fp64)):
+        solver.begin_run(q0, math.inf)
+        c = solver.advance(PRECISION_STEPS)
+        states[name] = solver.download(solver.state_tensor())
+        defect = solver.integrate(states[name]) - solver.integrate(q0) + np.array(c.flux_integral[:])
+        conservation[name] = {"mass_defect": float(defect[0]), "energy_defect": float(defect[3]),
+                              "time": float(c.time), "steps": int(c.steps)}
+    l1 = l1_density(fp32, states["fp32_mixed"], states["fp64"])
+    linf = float(np.abs(states["fp32_mixed"][..., 0] - states["fp64"][..., 0]).max())
     state_bytes = q0.numel() * 8
     line = {
         "metric": METRIC,
@@ -458,9 +464,9 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "l1_rho_vs_fp64": l1,
         "linf_rho_vs_fp64": linf,
         "conservation": conservation,
-        "precision_note": "FP32-mixed and FP64 states after the same number of steps, each with its own device CFL "
-                          "steps (end times in `conservation`); defects = final - initial integral + time-integrated "
-                          "boundary flux",
+        "precision_note": f"FP32-mixed and FP64 states after {PRECISION_STEPS} steps of the run loop from the "
+                          "workload's state, each with its own device CFL steps (end times in `conservation`); "
+                          "defects = final - initial integral + time-integrated boundary flux",
         "timing": {"repeats": results["fp32_mixed"]["repeats"], "block_steps": steps,
                    "block_ms_fp32_mixed": [round(v, 4) for v in results["fp32_mixed"]["block_ms"]],
                    "note": "each block times exactly `steps` RK3 steps (barrier + synchronise on both sides); "
@@ -579,8 +585,7 @@ def run_adjoint(args) -> dict:
     g = runner.pack(torch.stack([case.weight] + [torch.zeros_like(case.weight)] * 3, dim=-1))
 
     def timed(fn, repeats=3):
-        fn()  # warm-up (eager)
-        fn()  # warm-up (captures the CUDA graphs)
+        fn()  # warm-up
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         start.record()
@@ -718,6 +723,8 @@ def main() -> None:
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing of the default line")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances timing of the default line")
+    ap.add_argument("--min-seconds", type=float, default=1.0,
+                    help="repeat the timed block of `steps` steps until the clock samples span this long (0: once)")
     ap.add_argument("--profile-form", choices=["fp32_mixed", "fp64"], default=None,
                     help="time only this form's steps and print a short line (for profiler captures)")
     ap.add_argument("--batch-count", type=int, default=256)

@@ -15,11 +15,6 @@ on, then walks it in reverse. Peak device memory is about
 ``checkpoint_every * (6 states + 18 doubles per element)`` plus the
 checkpoints.
 
-Launches: at the sizes of a sensitivity study every kernel is short, so the
-forward pass and each backward segment (recompute with the tape + adjoint
-steps) are captured once in CUDA graphs on fixed buffers and replayed
-(``graphs=True``, the default); the first call of each runs eagerly.
-
 ``differentiable_run(runner, q0, bc_states)`` wraps this in a
 ``torch.autograd.Function``: q0 (Np, K, 4) and the fixed exterior states
 (rows, 4) are differentiable inputs, the final state (Np, K, 4) the output.
@@ -39,8 +34,7 @@ from .solver import EulerSolver, SolverError, _stream
 class AdjointRun:
     """Fixed-schedule run of ``solver`` and its discrete adjoint."""
 
-    def __init__(self, solver: EulerSolver, dts, *, checkpoint_every: int = 20, hold_theta: bool = False,
-                 graphs: bool = True):
+    def __init__(self, solver: EulerSolver, dts, *, checkpoint_every: int = 20, hold_theta: bool = False):
         import torch
 
         if checkpoint_every < 1:
@@ -67,11 +61,6 @@ class AdjointRun:
         self._work = torch.empty(int(self._lib.cfd_adjoint_work_bytes(ld, prec)), dtype=torch.uint8,
                                  device=self.ops.device)
         self._stage = torch.zeros(self._state_shape, dtype=solver._ws.dtype, device=self.ops.device)
-        self.graphs = bool(graphs)
-        self._fwd = None  # (graph, input buffer, final-state buffer, {step: checkpoint buffer})
-        self._bwd: dict = {}  # (segment start, with_boundary) -> graph
-        self._bwd_bufs = None
-        self._warm = {"forward": False, "backward": False}
 
     # ---- plumbing ------------------------------------------------------------
     def _new_state(self):
@@ -114,66 +103,17 @@ class AdjointRun:
         self.ops.bc_states.copy_(bc)
 
     # ---- forward / backward ----------------------------------------------------
-    def _forward_into(self, cur, nxt, ckpt: dict):
-        """The schedule's steps from `cur` (ping-pong with `nxt`), copying the
-        checkpoint states into ckpt[step]; returns the buffer of the final state."""
+    def forward(self, x0):
+        """Advance x0 (device layout) through the schedule. Returns the final
+        state and the checkpoints {step: state}."""
+        cur, nxt = x0.clone(), self._new_state()
+        checkpoints = {0: x0.clone()}
         for i in range(self.steps):
             self._step(cur, nxt, i)
             cur, nxt = nxt, cur
             if (i + 1) % self.checkpoint_every == 0 and i + 1 < self.steps:
-                ckpt[i + 1].copy_(cur)
-        return cur
-
-    def _capture(self, fn):
-        import torch
-
-        side = torch.cuda.Stream()
-        side.wait_stream(torch.cuda.current_stream())
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=side):
-            out = fn()
-        torch.cuda.current_stream().wait_stream(side)
-        return g, out
-
-    def forward(self, x0):
-        """Advance x0 (device layout) through the schedule. Returns the final
-        state and the checkpoints {step: state}."""
-        marks = [i + 1 for i in range(self.steps) if (i + 1) % self.checkpoint_every == 0 and i + 1 < self.steps]
-        if not (self.graphs and self._warm["forward"]):
-            self._warm["forward"] = True
-            ckpt = {s: self._new_state() for s in marks}
-            final = self._forward_into(x0.clone(), self._new_state(), ckpt)
-            return final, {0: x0.clone(), **ckpt}
-        if self._fwd is None:
-            a, b = self._new_state(), self._new_state()
-            ckpt = {s: self._new_state() for s in marks}
-            graph, final = self._capture(lambda: self._forward_into(a, b, ckpt))
-            self._fwd = (graph, a, final, ckpt)
-        graph, a, final, ckpt = self._fwd
-        a.copy_(x0)
-        graph.replay()
-        return final.clone(), {0: x0.clone(), **{s: c.clone() for s, c in ckpt.items()}}
-
-    def _segment(self, start: int, bufs, with_boundary: bool) -> None:
-        """Recompute steps start..stop-1 with the tape from bufs["states"][0],
-        then the adjoint steps in reverse: bufs["g"] in, bufs["g"] out."""
-        n = self.checkpoint_every
-        stop = min(start + n, self.steps)
-        seg, tapes, out = bufs["states"], bufs["tapes"], bufs["out"]
-        for i in range(start, stop):
-            j = i - start
-            dst = seg[j + 1] if j + 1 < n and i + 1 < stop else out
-            self._step(seg[j], dst, i, tapes[j])
-        g, g_next = bufs["g"], bufs["g_tmp"]
-        for i in reversed(range(start, stop)):
-            j = i - start
-            _native.check(self._lib.cfd_rk3_step_adjoint(
-                C.byref(self.solver.native), seg[j].data_ptr(), tapes[j].data_ptr(), self._dt(i),
-                g.data_ptr(), g_next.data_ptr(), bufs["bc_bar"].data_ptr() if with_boundary else None,
-                _native.ADJ_HOLD_THETA if self.hold_theta else 0, self._work.data_ptr(), _stream()))
-            g, g_next = g_next, g
-        if g is not bufs["g"]:
-            bufs["g"].copy_(g)
+                checkpoints[i + 1] = cur.clone()
+        return cur, checkpoints
 
     def backward(self, g_final, checkpoints, *, with_boundary: bool = True):
         """Adjoint of the final state (device layout) -> adjoint of the initial
@@ -181,27 +121,28 @@ class AdjointRun:
         import torch
 
         dev = self.ops.device
+        bc_bar = torch.zeros(self.ops.bc_states.shape, dtype=torch.float64, device=dev)
         n = self.checkpoint_every
-        if self._bwd_bufs is None:
-            self._bwd_bufs = {"states": [self._new_state() for _ in range(n)],
-                              "tapes": torch.empty((n, self._tape_bytes), dtype=torch.uint8, device=dev),
-                              "out": self._new_state(), "g": self._new_state(), "g_tmp": self._new_state(),
-                              "bc_bar": torch.zeros(self.ops.bc_states.shape, dtype=torch.float64, device=dev)}
-        bufs = self._bwd_bufs
-        bufs["bc_bar"].zero_()
-        bufs["g"].copy_(g_final)
-        use_graphs = self.graphs and self._warm["backward"]
-        self._warm["backward"] = True
-        for start in reversed(range(0, self.steps, n)):
-            bufs["states"][0].copy_(checkpoints[start])
-            if not use_graphs:
-                self._segment(start, bufs, with_boundary)
-                continue
-            key = (start, with_boundary)
-            if key not in self._bwd:
-                self._bwd[key] = self._capture(lambda: self._segment(start, bufs, with_boundary))[0]
-            self._bwd[key].replay()
-        return bufs["g"].clone(), bufs["bc_bar"].clone()
+        seg_states = [self._new_state() for _ in range(n)]
+        tapes = torch.empty((n, self._tape_bytes), dtype=torch.uint8, device=dev)
+        out = self._new_state()
+        g, g_next = g_final.clone(), self._new_state()
+        starts = list(range(0, self.steps, n))
+        for start in reversed(starts):
+            stop = min(start + n, self.steps)
+            seg_states[0].copy_(checkpoints[start])
+            for i in range(start, stop):
+                j = i - start
+                dst = seg_states[j + 1] if j + 1 < n and i + 1 < stop else out
+                self._step(seg_states[j], dst, i, tapes[j])
+            for i in reversed(range(start, stop)):
+                j = i - start
+                _native.check(self._lib.cfd_rk3_step_adjoint(
+                    C.byref(self.solver.native), seg_states[j].data_ptr(), tapes[j].data_ptr(), self._dt(i),
+                    g.data_ptr(), g_next.data_ptr(), bc_bar.data_ptr() if with_boundary else None,
+                    _native.ADJ_HOLD_THETA if self.hold_theta else 0, self._work.data_ptr(), _stream()))
+                g, g_next = g_next, g
+        return g, bc_bar
 
 
 def cfl_schedule(solver: EulerSolver, q0, *, steps: int | None = None, final_time: float | None = None) -> np.ndarray:
