@@ -56,12 +56,13 @@ FALLBACK_HBM_GBS = 6650.0
 # + dt_geo in stage 3). Neighbour-trace gathers are counted once (in the
 # neighbour's own read).
 # DRAM bytes per element of each stage launch (dram__bytes_read.sum +
-# dram__bytes_write.sum) measured by ncu on the tiled stage kernel at 512x512
-# quads (K = 524,288; the 724x724 workload is too large for a full capture),
+# dram__bytes_write.sum) measured by ncu on the autotuned stage kernels (FP32
+# shape 9, FP64 shape 5) at 512x512 quads (K = 524,288; the 724x724 workload
+# is too large for a full capture),
 # scaled to a launch of the benchmark by its element count (traffic grows in
 # proportion to K). Writes still in L2 when a launch ends are not counted
 # there, so the stage result's 240 / 480 B appear partly.
-NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (481.5, 739.6, 747.7), "fp64": (1007.6, 1515.6, 1521.4)}
+NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (480.7, 739.9, 750.1), "fp64": (1008.8, 1523.9, 1527.1)}
 
 
 def stage_bytes(real_bytes: int) -> list[int]:

@@ -179,19 +179,53 @@ __global__ void unpack_kernel(const R* __restrict__ in, double* __restrict__ out
 }
 
 template <typename R>
-__global__ void averages_kernel(CfdMesh m, const R* __restrict__ q, double* avg, double* integral) {
+__global__ void averages_kernel(CfdMesh m, const R* __restrict__ q, double* avg) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= m.num_elements) return;
   const int ld = m.ld;
-  const int inst = m.instance ? m.instance[e] : 0;
-  if (inst < 0) return;  // padding between instances
+  if (m.instance && m.instance[e] < 0) return;  // padding between instances
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     double s = 0.0;
 #pragma unroll
-    for (int i = 0; i < NP; ++i) s = fma(avg ? tab::AVG_W[i] : tab::CELL_W[i], (double)q[(c * NP + i) * ld + e], s);
-    if (avg) avg[c * ld + e] = s;
-    else atomicAdd(&integral[inst * 4 + c], m.jacobian[e] * s);  // dg.py:174-176
+    for (int i = 0; i < NP; ++i) s = fma(tab::AVG_W[i], (double)q[(c * NP + i) * ld + e], s);
+    avg[c * ld + e] = s;
+  }
+}
+
+// Domain integral per instance (dg.py:174-176): J_k sum_i w_i q_ik, summed
+// over the warp before one atomic per warp and variable when the warp's
+// elements belong to one instance (one atomic per element would serialise
+// on the four addresses).
+template <typename R>
+__global__ void integral_kernel(CfdMesh m, const R* __restrict__ q, double* integral) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ld = m.ld;
+  int inst = (e < m.num_elements) ? (m.instance ? m.instance[e] : 0) : -1;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  if (inst >= 0) {
+    const double jac = m.jacobian[e];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) s = fma(tab::CELL_W[i], (double)q[(c * NP + i) * ld + e], s);
+      v[c] = jac * s;
+    }
+  }
+  const int lane = threadIdx.x & 31;
+  const int first = __reduce_max_sync(0xffffffffu, (unsigned)(inst + 1)) - 1;  // an instance present in the warp
+  const bool uniform = __all_sync(0xffffffffu, inst < 0 || inst == first) && first >= 0;
+  if (uniform) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    }
+    if (lane == 0)
+      for (int c = 0; c < 4; ++c) atomicAdd(&integral[first * 4 + c], v[c]);
+  } else if (inst >= 0) {
+    for (int c = 0; c < 4; ++c) atomicAdd(&integral[inst * 4 + c], v[c]);
   }
 }
 
@@ -451,8 +485,8 @@ int cfd_cell_averages(const CfdSolver* s, const void* q, double* avg, void* stre
   if (!q || !avg) return fail(CFD_E_ARG, "cfd_cell_averages: null pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const unsigned g = blocks_for(s->mesh.num_elements, 128);
-  if (s->precision == CFD_FP64) averages_kernel<double><<<g, 128, 0, st>>>(s->mesh, (const double*)q, avg, nullptr);
-  else averages_kernel<float><<<g, 128, 0, st>>>(s->mesh, (const float*)q, avg, nullptr);
+  if (s->precision == CFD_FP64) averages_kernel<double><<<g, 128, 0, st>>>(s->mesh, (const double*)q, avg);
+  else averages_kernel<float><<<g, 128, 0, st>>>(s->mesh, (const float*)q, avg);
   return check_launch("cfd_cell_averages");
 }
 
@@ -464,8 +498,8 @@ int cfd_integrate(const CfdSolver* s, const void* q, double* integral, void* str
   if (cudaMemsetAsync(integral, 0, sizeof(double) * 4 * s->mesh.num_instances, st) != cudaSuccess)
     return check_launch("cfd_integrate: memset");
   const unsigned g = blocks_for(s->mesh.num_elements, 128);
-  if (s->precision == CFD_FP64) averages_kernel<double><<<g, 128, 0, st>>>(s->mesh, (const double*)q, nullptr, integral);
-  else averages_kernel<float><<<g, 128, 0, st>>>(s->mesh, (const float*)q, nullptr, integral);
+  if (s->precision == CFD_FP64) integral_kernel<double><<<g, 128, 0, st>>>(s->mesh, (const double*)q, integral);
+  else integral_kernel<float><<<g, 128, 0, st>>>(s->mesh, (const float*)q, integral);
   return check_launch("cfd_integrate");
 }
 

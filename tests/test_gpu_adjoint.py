@@ -260,32 +260,32 @@ def test_sod_400x40_200_steps_sensitivity(report):
     assert abs(adjoint - central) < 3 * spread + 1e-4 * abs(central)
 
 
-def _smooth_bump_direction(case, seed, modulated):
-    """A random smooth perturbation of all four conserved variables carried
-    by the density bump's Gaussian envelope (random coefficients per
-    variable; with `modulated`, times a random smooth wave along the tube),
-    so that it is smooth where the solution is smooth and vanishes where the
-    solution is flat: the forward map is differentiable along it."""
-    x, y = (torch.as_tensor(a, device=case.solver.operators.device) for a in case.solver.node_coordinates())
+def _smooth_bump_direction(case, seed):
+    """A random smooth density perturbation inside the bump: the bump's
+    Gaussian envelope times a random smooth modulation along the tube
+    (random amplitude, wavelength and phase). The initial velocity is zero
+    and the pressure is untouched, so the perturbation is a density (entropy)
+    profile in the region where the solution already varies smoothly, and it
+    vanishes where the solution is flat: the forward map is differentiable
+    along it (a perturbation of a flat region would switch the troubled-cell
+    detector, whose threshold is 1e-10 |average|)."""
+    x = torch.as_tensor(case.solver.node_coordinates()[0], device=case.solver.operators.device)
     gen = np.random.default_rng(seed)
-    env = case.bump / case.amplitude
-    d = torch.zeros(case.solver.state_shape, dtype=torch.float64, device=env.device)
-    for c in range(4):
-        a, b, phase = gen.uniform(-1, 1), gen.uniform(-1, 1), gen.uniform(0, 2 * np.pi)
-        wave = torch.sin(2 * np.pi * (x - case.bump_center) / 0.2 + phase) if modulated else 0.0
-        d[..., c] = env * (a + b * wave)
+    b, wavelength, phase = gen.uniform(-0.8, 0.8), gen.uniform(0.1, 0.3), gen.uniform(0, 2 * np.pi)
+    d = torch.zeros(case.solver.state_shape, dtype=torch.float64, device=x.device)
+    d[..., 0] = case.bump / case.amplitude * (1.0 + b * torch.sin(2 * np.pi * (x - case.bump_center) / wavelength + phase))
     return d
 
 
-@pytest.mark.parametrize("seed,modulated", [(1, False), (2, False), (3, True)])
-def test_sod_400x40_random_smooth_direction(seed, modulated, report):
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_sod_400x40_random_smooth_direction(seed, report):
     """Config 3 (Sod 400x40, 200 steps, checkpoints every 20): <dJ/dq0, d>
-    for random smooth directions d in the bump region, all four conserved
-    variables, against the central difference (eps = 1e-6) to 1e-4."""
+    for random smooth density directions d in the bump region, against the
+    central difference (eps = 1e-6) to 1e-4."""
     case, runner = _sod_case(400, 40, 200, 20, seed=0)
-    d = _smooth_bump_direction(case, seed, modulated)
+    d = _smooth_bump_direction(case, seed)
     ad, central, fourth, _ = _direction(case, runner, d)
-    report(f"adjoint Sod 400x40 200 steps, random smooth direction (seed {seed}, modulated {modulated}): {ad:.10e}, "
+    report(f"adjoint Sod 400x40 200 steps, random smooth density direction (seed {seed}): {ad:.10e}, "
            f"rel to central(1e-6) {_rel(ad, central):.1e}, to 4th-order(1e-4) {_rel(ad, fourth):.1e}")
     assert _rel(ad, central) < 1e-4
 
