@@ -63,6 +63,12 @@ FALLBACK_HBM_GBS = 6650.0
 # proportion to K). Writes still in L2 when a launch ends are not counted
 # there, so the stage result's 240 / 480 B appear partly.
 NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (480.7, 739.9, 750.1), "fp64": (1008.8, 1523.9, 1527.1)}
+# Warp instructions issued per element of each stage launch (ncu
+# smsp__inst_executed.sum / K, same captures). With 148 SMs issuing at most
+# 4 warp instructions per cycle each, they bound a launch from below at
+# instructions / (148 * 4 * SM clock): the instruction-issue roofline.
+NCU_WARP_INSTRUCTIONS_PER_ELEMENT = {"fp32_mixed": (267.1, 289.7, 305.5), "fp64": (518.1, 533.1, 587.3)}
+SMS, ISSUE_PER_SM_CYCLE = 148, 4
 
 
 def stage_bytes(real_bytes: int) -> list[int]:
@@ -355,21 +361,21 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     forms = (("fp32_mixed", fp32), ("fp64", fp64))
     if args.profile_form:  # one form's timed steps only: the command line of the profiler captures
         forms = tuple(f for f in forms if f[0] == args.profile_form)
+    props = torch.cuda.get_device_properties(dev)
+    # nvidia-smi prints the PCI address as dddddddd:bb:dd.f
+    bus = "%08x:%02x:%02x" % (int(getattr(props, "pci_domain_id", 0) or 0),
+                              int(getattr(props, "pci_bus_id", 0) or 0),
+                              int(getattr(props, "pci_device_id", 0) or 0))
     for name, solver in forms:
         solver.begin_run(q0, math.inf)
-        if name == "fp32_mixed":
-            props = torch.cuda.get_device_properties(dev)
-            # nvidia-smi prints the PCI address as dddddddd:bb:dd.f
-            bus = "%08x:%02x:%02x" % (int(getattr(props, "pci_domain_id", 0) or 0),
-                                      int(getattr(props, "pci_bus_id", 0) or 0),
-                                      int(getattr(props, "pci_device_id", 0) or 0))
-            sampler = ClockSampler(bus)
-            with sampler:
+        sampler = ClockSampler(bus)
+        with sampler:
+            if name == "fp32_mixed":
                 r = timed_steps(solver, steps, warmup, world, sampler=sampler, min_seconds=args.min_seconds)
-            r["clocks"] = sampler.summary()
-        else:
-            r = timed_steps(solver, steps, warmup, world, min_seconds=args.min_seconds,
-                            repeats=results["fp32_mixed"]["repeats"] if "fp32_mixed" in results else None)
+            else:
+                r = timed_steps(solver, steps, warmup, world, sampler=sampler, min_seconds=args.min_seconds,
+                                repeats=results["fp32_mixed"]["repeats"] if "fp32_mixed" in results else None)
+        r["clocks"] = sampler.summary()
         results[name] = r
 
     if args.profile_form:
@@ -418,6 +424,17 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                                          f"{round(sum(sb) * k / 3)}",
                          "peak_source": peak_kind, "algorithmic_bytes_per_element_step": sum(sb)},
         }
+        mhz = r["clocks"].get("sm_mhz") if r.get("clocks") else None
+        if mhz:
+            inst = NCU_WARP_INSTRUCTIONS_PER_ELEMENT[name]
+            bound_s = [n * k / (SMS * ISSUE_PER_SM_CYCLE * mhz * 1e6) for n in inst]
+            out[name]["issue_roofline"] = {
+                "warp_instructions_per_element": list(inst), "sm_mhz": mhz,
+                "bound_ms": [round(1e3 * b, 4) for b in bound_s],
+                "frac": round(sum(bound_s) / sum(stage_s), 4),
+                "note": "instruction-issue bound of the three stage launches (148 SMs x 4 warp instructions per "
+                        "cycle at the median SM clock of the timed region; instruction counts from ncu at "
+                        "K=524,288, per element) over their CUDA-event time"}
     # precision: both forms advance the same state by PRECISION_STEPS steps of
     # the run loop (each with its own device CFL steps), untimed
     states, conservation = {}, {}
@@ -458,9 +475,12 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                              for n, t in tuned.items()},
         },
         "roofline": out["fp32_mixed"]["roofline"],
+        "issue_roofline": out["fp32_mixed"].get("issue_roofline"),
         "stage_ms": out["fp32_mixed"]["stage_ms"],
         "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms_per_step"],
-                 "stage_ms": out["fp64"]["stage_ms"], "roofline": out["fp64"]["roofline"], "dtype": "f64"},
+                 "stage_ms": out["fp64"]["stage_ms"], "roofline": out["fp64"]["roofline"],
+                 "issue_roofline": out["fp64"].get("issue_roofline"), "dtype": "f64",
+                 "clocks": results["fp64"].get("clocks")},
         "fp32_over_fp64": out["fp32_mixed"]["value"] / out["fp64"]["value"],
         "l1_rho_vs_fp64": l1,
         "linf_rho_vs_fp64": linf,
@@ -480,6 +500,9 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "gpu_launches": 6 * steps,
         "clocks": results["fp32_mixed"]["clocks"],
     }
+    if line["clocks"].get("sm_mhz"):
+        # time x clock: comparable across runs at different SM clocks
+        line["clocks"]["kcycles_per_step"] = round(line["ms_per_step"] * line["clocks"]["sm_mhz"], 1)
     return line
 
 

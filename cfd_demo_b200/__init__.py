@@ -7,17 +7,19 @@ Same public names as ``cfd_demo``; ``SolverConfig`` adds ``precision``
 ("fp64" plain form, "fp32_mixed").
 """
 
-from .boundary import FixedState, SlipWall
-from .cases import SodShockTube, sod_shock_tube
+from .boundary import ExactState, FixedState, SlipWall
+from .cases import ObliqueShockCase, SodShockTube, oblique_shock, sod_shock_tube
 from .fluxes import INTERFACE_FLUXES, get_interface_flux
 from .limiters import LIMITER_FUNCTIONS, get_limiter_function
-from .mesh import TriangleMesh, jittered_rectangle_mesh, rectangle_mesh
+from .mesh import TriangleMesh, jittered_rectangle_mesh, rectangle_mesh, sheared_rectangle_mesh
 from .solver import EulerSolver, RunResult, SolverConfig, SolverError, StepReport
 
 __all__ = [
     "INTERFACE_FLUXES",
     "LIMITER_FUNCTIONS",
+    "ObliqueShockCase",
     "EulerSolver",
+    "ExactState",
     "FixedState",
     "RunResult",
     "SlipWall",
@@ -29,6 +31,8 @@ __all__ = [
     "get_interface_flux",
     "get_limiter_function",
     "jittered_rectangle_mesh",
+    "oblique_shock",
     "rectangle_mesh",
+    "sheared_rectangle_mesh",
     "sod_shock_tube",
 ]

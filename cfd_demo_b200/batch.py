@@ -84,7 +84,8 @@ class BatchedEulerSolver:
             conn = build_connectivity(case.mesh)
             geo = element_geometry(case.mesh)
             kind, state = resolve_boundary_conditions(conn, case.boundary_conditions)
-            parts.append(host_tables(case.mesh, conn, geo, self.reference, kind, state, device=device))
+            parts.append(host_tables(case.mesh, conn, geo, self.reference, kind, state, device=device,
+                                     boundary_conditions=case.boundary_conditions))
         self.precision = PRECISIONS[config.precision]
         self.operators = DeviceTables(parts, device, self.precision)
         self._ws = Workspace(self.operators, self.precision, config.limiter != "unlimited")

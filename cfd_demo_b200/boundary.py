@@ -9,6 +9,7 @@ import numpy as np
 
 SLIP_WALL = 1
 FIXED_STATE = 2
+EXACT_STATE = 3
 
 
 @dataclass(frozen=True)
@@ -38,4 +39,35 @@ class FixedState:
         return cls((rho, rho * u, rho * v, energy))
 
 
-BoundaryCondition = SlipWall | FixedState
+@dataclass(frozen=True, eq=False)
+class ExactState:
+    """Exterior states from a known solution (CFD-demo's proposed ADR 0012,
+    docs/adr/0012-...:32-46): `function(x, y)` maps arrays of physical
+    coordinates to conserved states of shape x.shape + (4,). It is evaluated
+    once, when the solver is built, at every face node of the tagged faces
+    (per-node exterior states of the interface flux), and its cell average
+    over each boundary element reflected across the boundary face is the
+    ghost average of the troubled-cell limiter: `cell_average(corners)`
+    ((n, 3, 2) triangles -> (n, 4)) when given, else the mean over the
+    centroids of 32 x 32 equal sub-triangles. For verification with an
+    analytic solution, not a general outflow condition."""
+
+    function: object
+    cell_average: object = None
+    kind: int = EXACT_STATE
+
+    def __post_init__(self) -> None:
+        if not callable(self.function):
+            raise ValueError("ExactState needs a callable function(x, y) -> conserved states.")
+        if self.cell_average is not None and not callable(self.cell_average):
+            raise ValueError("ExactState cell_average must be callable (or None).")
+
+    def states(self, x: np.ndarray, y: np.ndarray) -> np.ndarray:
+        x, y = np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)
+        q = np.asarray(self.function(x, y), dtype=np.float64)
+        if q.shape != x.shape + (4,) or not np.all(np.isfinite(q)):
+            raise ValueError("ExactState function must return finite conserved states of shape x.shape + (4,).")
+        return q
+
+
+BoundaryCondition = SlipWall | FixedState | ExactState

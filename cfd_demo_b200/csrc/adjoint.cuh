@@ -174,6 +174,7 @@ struct AdjParams {
   int hold_theta;      // 1: pressure-scaling theta constant (jax.grad semantics)
   int* list;           // elements that need the full limiter replay [ld]
   int* count;          // their number
+  uint8_t* listed;     // per element: 1 if listed (qtb holds its adjoint), 0 if qt_bar = g [ld]
 };
 
 __device__ __forceinline__ int element_instance(const CfdMesh& m, int e) { return m.instance ? m.instance[e] : 0; }
@@ -237,7 +238,7 @@ __device__ __forceinline__ void adj_limit_decide(const AdjParams& P, int e, doub
         na[2] = xsub(a[2], xmul(xmul(2.0, mn), ny));
         na[3] = a[3];
       } else {
-        const int row = m.neighbor[f * ld + e];
+        const int row = m.neighbor[f * ld + e] + (kind == CFD_FACE_EXACT_STATE ? NFP : 0);
 #pragma unroll
         for (int c = 0; c < 4; ++c) na[c] = m.bc_states[row * 4 + c];
       }
@@ -269,13 +270,13 @@ __device__ __forceinline__ void adj_limit_decide(const AdjParams& P, int e, doub
 }
 
 // Light pass over every element: where the limiters left the element as it
-// was, qt_bar = g and the neighbour-average adjoints are zero; the others
-// (troubled or positivity-scaled, a small minority) are listed for
-// adj_limit_heavy_kernel.
+// was, qt_bar = g and the neighbour-average adjoints are zero, which the
+// consumers read from g and from the listed flags instead of a copy; the
+// others (troubled or positivity-scaled, a small minority) are flagged and
+// listed for adj_limit_heavy_kernel.
 template <typename R, int PHI>
 __global__ void __launch_bounds__(128) adj_limit_scan_kernel(const AdjParams P) {
   const CfdMesh& m = P.m;
-  const int ld = m.ld;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = e < m.num_elements && element_instance(m, e) >= 0;
   bool listed = false;
@@ -287,22 +288,36 @@ __global__ void __launch_bounds__(128) adj_limit_scan_kernel(const AdjParams P) 
     listed = troubled || need_pos;
   }
   warp_list_append(P.list, P.count, listed, e);  // every lane of the warp takes part
-  if (!live || listed) return;
-  const R* __restrict__ g = (const R*)P.g;
-  R* __restrict__ qtb = (R*)P.qtb;
-#pragma unroll 4
-  for (int k = 0; k < 4 * NP; ++k) qtb[k * ld + e] = g[k * ld + e];
-  if (PHI != LIM_UNLIMITED) {
-    R* __restrict__ nab = (R*)P.nab;
+  if (e < m.ld) P.listed[e] = listed ? 1 : 0;
+}
+
+// Whether element e's qt_bar lives in qtb (written by the heavy pass for a
+// listed element, or by adj_lift_kernel when a listed neighbour added the
+// adjoint of this element's average) rather than being g itself. Every
+// consumer evaluates the same predicate.
+__device__ __forceinline__ bool adj_uses_qtb(const AdjParams& P, int e) {
+  if (P.listed[e]) return true;
+  if (!P.limited) return false;
+  const CfdMesh& m = P.m;
+  const int finfo = m.face_info[e];
+  bool any = false;
 #pragma unroll
-    for (int k = 0; k < 12; ++k) nab[k * ld + e] = R(0);
-  }
+  for (int f = 0; f < 3; ++f)
+    if (((finfo >> (8 * f)) & 3) == CFD_FACE_INTERIOR) any |= P.listed[m.neighbor[f * m.ld + e]] != 0;
+  return any;
 }
 
 // qt_bar = Lambda'(qt)^T g for one listed element, plus the adjoints of the
 // three neighbour / ghost averages it read (gathered by adj_lift_kernel).
+// Four lanes of a warp share the element, lane c (= lane % 4) owning
+// conserved variable c: the troubled-cell reconstruction and its reverse are
+// separate per variable; the positivity scalings couple the variables through
+// the density minimum, the scaling thetas and the pressure gradient at the
+// critical node, which the quad exchanges with shuffles under its own mask
+// (the four lanes always take the same branches: every decision is made from
+// values they share).
 template <typename R, int PHI>
-__device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
+__device__ __forceinline__ void adj_limit_quad(const AdjParams& P, int e, int c, unsigned qmask, int base) {
   const CfdMesh& m = P.m;
   const int ld = m.ld;
   const R* __restrict__ qt = (const R*)P.qt;
@@ -315,59 +330,59 @@ __device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
   R scaled[3][4];
   bool troubled, need_pos;
   adj_limit_decide<R, PHI>(P, e, a, eps, pt, scaled, troubled, need_pos);
+  const double ac_d = c == 0 ? a[0] : (c == 1 ? a[1] : (c == 2 ? a[2] : a[3]));
+  R sc[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) sc[f] = c == 0 ? scaled[f][0] : (c == 1 ? scaled[f][1] : (c == 2 ? scaled[f][2] : scaled[f][3]));
 
-  R s[NP][4];
+  R s[NP];
 #pragma unroll
-  for (int i = 0; i < NP; ++i)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) s[i][c] = qt[(c * NP + i) * ld + e];
-  // --- forward troubled-cell reconstruction, keeping what the reverse needs
-  R proj[3][4], mfac[3][4], del[3][4], thp[4], thn[4], pos[4], neg[4];
+  for (int i = 0; i < NP; ++i) s[i] = qt[(c * NP + i) * ld + e];
+  // --- forward troubled-cell reconstruction of variable c, keeping what the reverse needs
+  R proj[3], mfac[3], del[3], thp = R(0), thn = R(0), pos = R(0), neg = R(0);
   if (troubled) {
+    const R ac = (R)ac_d;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const R ac = (R)a[c];
+    for (int f = 0; f < 3; ++f) {
+      R pr = xmul((R)tab::P1MID[f][0], s[0]);
 #pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        R pr = xmul((R)tab::P1MID[f][0], s[0][c]);
-#pragma unroll
-        for (int i = 1; i < NP; ++i) pr = xadd(pr, xmul((R)tab::P1MID[f][i], s[i][c]));
-        pr = xsub(pr, ac);
-        proj[f][c] = pr;
-        R d = R(0), mf = R(0);
-        if (pr != R(0)) {
-          mf = jmin(R(1), phi<R, PHI>(xdiv(scaled[f][c], pr)));
-          d = xmul(pr, mf);
-        }
-        mfac[f][c] = mf;
-        del[f][c] = d;
-        pos[c] = f == 0 ? jmax(d, R(0)) : xadd(pos[c], jmax(d, R(0)));
-        neg[c] = f == 0 ? jmax(-d, R(0)) : xadd(neg[c], jmax(-d, R(0)));
+      for (int i = 1; i < NP; ++i) pr = xadd(pr, xmul((R)tab::P1MID[f][i], s[i]));
+      pr = xsub(pr, ac);
+      proj[f] = pr;
+      R d = R(0), mf = R(0);
+      if (pr != R(0)) {
+        mf = jmin(R(1), phi<R, PHI>(xdiv(sc[f], pr)));
+        d = xmul(pr, mf);
       }
-      thp[c] = pos[c] > R(0) ? jmin(R(1), xdiv(neg[c], pos[c])) : R(0);
-      thn[c] = neg[c] > R(0) ? jmin(R(1), xdiv(pos[c], neg[c])) : R(0);
-      R dl[3];
+      mfac[f] = mf;
+      del[f] = d;
+      pos = f == 0 ? jmax(d, R(0)) : xadd(pos, jmax(d, R(0)));
+      neg = f == 0 ? jmax(-d, R(0)) : xadd(neg, jmax(-d, R(0)));
+    }
+    thp = pos > R(0) ? jmin(R(1), xdiv(neg, pos)) : R(0);
+    thn = neg > R(0) ? jmin(R(1), xdiv(pos, neg)) : R(0);
+    R dl[3];
 #pragma unroll
-      for (int f = 0; f < 3; ++f)
-        dl[f] = xsub(xmul(thp[c], jmax(del[f][c], R(0))), xmul(thn[c], jmax(-del[f][c], R(0))));
+    for (int f = 0; f < 3; ++f) dl[f] = xsub(xmul(thp, jmax(del[f], R(0))), xmul(thn, jmax(-del[f], R(0))));
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        R v = xmul((R)tab::LINBASIS[i][0], dl[0]);
-        v = xadd(v, xmul((R)tab::LINBASIS[i][1], dl[1]));
-        v = xadd(v, xmul((R)tab::LINBASIS[i][2], dl[2]));
-        s[i][c] = xadd(ac, v);
-      }
+    for (int i = 0; i < NP; ++i) {
+      R v = xmul((R)tab::LINBASIS[i][0], dl[0]);
+      v = xadd(v, xmul((R)tab::LINBASIS[i][1], dl[1]));
+      v = xadd(v, xmul((R)tab::LINBASIS[i][2], dl[2]));
+      s[i] = xadd(ac, v);
     }
   }
-  // --- forward positivity decisions (the order of positivity() in kernels.cu)
+  // --- forward positivity decisions (the order of positivity() in kernels.cu);
+  // the density minimum comes from lane 0 of the quad
   int imin = 0;
-  double rmin = (double)s[0][0];
+  double rmin = (double)s[0];
 #pragma unroll
   for (int i = 1; i < NP; ++i) {
-    const double r = (double)s[i][0];
+    const double r = (double)s[i];
     imin = r < rmin ? i : imin;
     rmin = jmin(rmin, r);
   }
+  rmin = __shfl_sync(qmask, rmin, base);
   double th1 = 1.0;
   bool dens = false, dclip = true;
   if (rmin < eps) {
@@ -376,9 +391,7 @@ __device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
     th1 = jmin(jmax(raw, 0.0), 1.0);
     dclip = !(raw > 0.0 && raw < 1.0);
 #pragma unroll
-    for (int i = 0; i < NP; ++i)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) s[i][c] = (R)xadd(a[c], xmul(th1, xsub((double)s[i][c], a[c])));
+    for (int i = 0; i < NP; ++i) s[i] = (R)xadd(ac_d, xmul(th1, xsub((double)s[i], ac_d)));
   }
   // the pressure-scaling theta and its critical node, as the forward
   // bisection found them (limit_kernel records them in the tape)
@@ -386,14 +399,12 @@ __device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
   const int i2 = (int)P.pos[ld + e];
   if (!(th2 < 1.0)) th2 = 1.0;
 
-  // --- reverse pass; y is the running adjoint of the nodal state, abar that
-  // of the cell averages (which are AVG_W-weighted sums of qt)
-  R y[NP][4];
+  // --- reverse pass; y is the running adjoint of the nodal values of
+  // variable c, abar that of its cell average (an AVG_W-weighted sum of qt)
+  R y[NP];
 #pragma unroll
-  for (int i = 0; i < NP; ++i)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) y[i][c] = g[(c * NP + i) * ld + e];
-  R abar[4] = {R(0), R(0), R(0), R(0)};
+  for (int i = 0; i < NP; ++i) y[i] = g[(c * NP + i) * ld + e];
+  R abar = R(0);
   // pressure scaling out = a + th2 (in - a). th2 is the bisection root of
   // p(a + th (in_i2 - a)) = pt at the critical node i2: held constant (the
   // derivative of the bisection itself), or differentiated implicitly,
@@ -401,174 +412,154 @@ __device__ __forceinline__ void adj_limit_element(const AdjParams& P, int e) {
   // z = a + th2 (in_i2 - a), which follows the root the bisection resolves to
   // 2^-60 (pt held constant, like eps).
   if (th2 < 1.0) {
-    R thbar = R(0);
+    R part = R(0), sum = R(0);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      R sum = R(0);
-#pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        thbar += (R)((double)s[i][c] - a[c]) * y[i][c];
-        sum += y[i][c];
-        y[i][c] *= (R)th2;
-      }
-      abar[c] += (R)(1.0 - th2) * sum;
+    for (int i = 0; i < NP; ++i) {
+      part += (R)((double)s[i] - ac_d) * y[i];
+      sum += y[i];
+      y[i] *= (R)th2;
     }
+    abar += (R)(1.0 - th2) * sum;
+    part += __shfl_xor_sync(qmask, part, 1);
+    const R thbar = part + __shfl_xor_sync(qmask, part, 2);
     if (!P.hold_theta && i2 >= 0) {
+      double dc = 0.0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) dc = (j == i2) ? (double)s[j] : dc;
+      dc -= ac_d;
       double d[4];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        double v = 0.0;
-#pragma unroll
-        for (int j = 0; j < NP; ++j) v = (j == i2) ? (double)s[j][c] : v;
-        d[c] = v - a[c];
-      }
+      for (int k = 0; k < 4; ++k) d[k] = __shfl_sync(qmask, dc, base + k);
       const double z0 = a[0] + th2 * d[0], u = (a[1] + th2 * d[1]) / z0, v = (a[2] + th2 * d[2]) / z0;
       const double gp[4] = {gm1 * 0.5 * (u * u + v * v), -gm1 * u, -gm1 * v, gm1};  // grad p(z)
       const double den = gp[0] * d[0] + gp[1] * d[1] + gp[2] * d[2] + gp[3] * d[3];
       if (den != 0.0) {
         const double k = -(double)thbar / den;
+        const double gpc = c == 0 ? gp[0] : (c == 1 ? gp[1] : (c == 2 ? gp[2] : gp[3]));
+        abar += (R)(k * (1.0 - th2) * gpc);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          abar[c] += (R)(k * (1.0 - th2) * gp[c]);
-#pragma unroll
-          for (int i = 0; i < NP; ++i)
-            if (i == i2) y[i][c] += (R)(k * th2 * gp[c]);
-        }
+        for (int i = 0; i < NP; ++i)
+          if (i == i2) y[i] += (R)(k * th2 * gpc);
       }
     }
   }
   // density scaling out = a + th1 (in - a), th1 = (a_rho - eps) / (a_rho - min_i rho_i)
   if (dens) {
-    R thbar = R(0);
+    R part = R(0), sum = R(0);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      R sum = R(0);
-#pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        const R din = th1 > 0.0 ? (R)(((double)s[i][c] - a[c]) / th1) : R(0);  // in - a
-        thbar += din * y[i][c];
-        sum += y[i][c];
-        y[i][c] *= (R)th1;
-      }
-      abar[c] += (R)(1.0 - th1) * sum;
+    for (int i = 0; i < NP; ++i) {
+      const R din = th1 > 0.0 ? (R)(((double)s[i] - ac_d) / th1) : R(0);  // in - a
+      part += din * y[i];
+      sum += y[i];
+      y[i] *= (R)th1;
     }
-    if (!dclip) {
+    abar += (R)(1.0 - th1) * sum;
+    part += __shfl_xor_sync(qmask, part, 1);
+    const R thbar = part + __shfl_xor_sync(qmask, part, 2);
+    if (!dclip && c == 0) {
       const double span = a[0] - rmin;
-      const R dth_da = (R)((eps - rmin) / (span * span));
+      abar += thbar * (R)((eps - rmin) / (span * span));
       const R dth_dmin = (R)((a[0] - eps) / (span * span));
-      abar[0] += thbar * dth_da;
 #pragma unroll
       for (int i = 0; i < NP; ++i)
-        if (i == imin) y[i][0] += thbar * dth_dmin;
+        if (i == imin) y[i] += thbar * dth_dmin;
     }
   }
   // troubled-cell reconstruction
-  R nabar[3][4];
-#pragma unroll
-  for (int f = 0; f < 3; ++f)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) nabar[f][c] = R(0);
+  R nabar[3] = {R(0), R(0), R(0)};
   if (troubled) {
     const R* __restrict__ cs = GeoPtr<R>::cs(m);
+    R ab = R(0), dpb[3] = {R(0), R(0), R(0)};
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      R ab = R(0), dpb[3] = {R(0), R(0), R(0)};
+    for (int i = 0; i < NP; ++i) {
+      ab += y[i];
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        ab += y[i][c];
-#pragma unroll
-        for (int f = 0; f < 3; ++f) dpb[f] += (R)tab::LINBASIS[i][f] * y[i][c];
-        y[i][c] = R(0);  // a rebuilt element depends on its nodes only through the P1 projections
-      }
-      R thpb = R(0), thnb = R(0), pb[3], nb_[3];
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        pb[f] = thp[c] * dpb[f];
-        nb_[f] = -thn[c] * dpb[f];
-        thpb += jmax(del[f][c], R(0)) * dpb[f];
-        thnb -= jmax(-del[f][c], R(0)) * dpb[f];
-      }
-      R posb = R(0), negb = R(0);
-      if (pos[c] > R(0) && neg[c] < pos[c]) {  // thp = neg / pos below the cap
-        negb += thpb / pos[c];
-        posb -= thpb * neg[c] / (pos[c] * pos[c]);
-      }
-      if (neg[c] > R(0) && pos[c] < neg[c]) {  // thn = pos / neg below the cap
-        posb += thnb / neg[c];
-        negb -= thnb * pos[c] / (neg[c] * neg[c]);
-      }
-      R difb[3] = {R(0), R(0), R(0)};
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        const R d = del[f][c];
-        const R delb = d > R(0) ? pb[f] + posb : (d < R(0) ? -(nb_[f] + negb) : R(0));
-        R projb = R(0), scb = R(0);
-        const R pr = proj[f][c];
-        if (pr != R(0)) {
-          projb = mfac[f][c] * delb;
-          const R r = scaled[f][c] / pr;
-          const R rb = phi<R, PHI>(r) < R(1) ? phi_grad<R, PHI>(r) * pr * delb : R(0);
-          scb = rb / pr;
-          projb -= rb * scaled[f][c] / (pr * pr);
-        }
-        // proj_f = P1MID_f . q - a ; scaled_f = 1.5 (alpha_f dif_f + beta_f dif_pf), dif = na - a
-        ab -= projb;
-#pragma unroll
-        for (int i = 0; i < NP; ++i) y[i][c] += (R)tab::P1MID[f][i] * projb;
-        const int pf = (finfo >> (8 * f + 4)) & 3;
-        const R al = cs[f * ld + e], be = cs[(3 + f) * ld + e];
-        difb[f] += (R)NEIGHBOR_FACTOR * al * scb;
-        const R t = (R)NEIGHBOR_FACTOR * be * scb;
-        if (pf == 0) difb[0] += t;
-        else if (pf == 1) difb[1] += t;
-        else difb[2] += t;
-      }
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        nabar[f][c] = difb[f];
-        ab -= difb[f];
-      }
-      abar[c] += ab;
+      for (int f = 0; f < 3; ++f) dpb[f] += (R)tab::LINBASIS[i][f] * y[i];
+      y[i] = R(0);  // a rebuilt element depends on its nodes only through the P1 projections
     }
-    // ghost averages: a slip wall mirrors this element's average; a fixed
-    // exterior state is a boundary parameter
+    R thpb = R(0), thnb = R(0), pb[3], nb_[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      pb[f] = thp * dpb[f];
+      nb_[f] = -thn * dpb[f];
+      thpb += jmax(del[f], R(0)) * dpb[f];
+      thnb -= jmax(-del[f], R(0)) * dpb[f];
+    }
+    R posb = R(0), negb = R(0);
+    if (pos > R(0) && neg < pos) {  // thp = neg / pos below the cap
+      negb += thpb / pos;
+      posb -= thpb * neg / (pos * pos);
+    }
+    if (neg > R(0) && pos < neg) {  // thn = pos / neg below the cap
+      posb += thnb / neg;
+      negb -= thnb * pos / (neg * neg);
+    }
+    R difb[3] = {R(0), R(0), R(0)};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const R d = del[f];
+      const R delb = d > R(0) ? pb[f] + posb : (d < R(0) ? -(nb_[f] + negb) : R(0));
+      R projb = R(0), scb = R(0);
+      const R pr = proj[f];
+      if (pr != R(0)) {
+        projb = mfac[f] * delb;
+        const R r = sc[f] / pr;
+        const R rb = phi<R, PHI>(r) < R(1) ? phi_grad<R, PHI>(r) * pr * delb : R(0);
+        scb = rb / pr;
+        projb -= rb * sc[f] / (pr * pr);
+      }
+      // proj_f = P1MID_f . q - a ; scaled_f = 1.5 (alpha_f dif_f + beta_f dif_pf), dif = na - a
+      ab -= projb;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) y[i] += (R)tab::P1MID[f][i] * projb;
+      const int pf = (finfo >> (8 * f + 4)) & 3;
+      const R al = cs[f * ld + e], be = cs[(3 + f) * ld + e];
+      difb[f] += (R)NEIGHBOR_FACTOR * al * scb;
+      const R t = (R)NEIGHBOR_FACTOR * be * scb;
+      if (pf == 0) difb[0] += t;
+      else if (pf == 1) difb[1] += t;
+      else difb[2] += t;
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      nabar[f] = difb[f];
+      ab -= difb[f];
+    }
+    abar += ab;
+    // ghost averages: a slip wall mirrors this element's average (the
+    // mirror couples the momentum lanes); a fixed exterior state is a
+    // boundary parameter
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       const int kind = (finfo >> (8 * f)) & 3;
       if (kind == CFD_FACE_SLIP_WALL) {
         const R nx = (R)m.face_geo[(3 * f) * ld + e], ny = (R)m.face_geo[(3 * f + 1) * ld + e];
-        const R dm = nabar[f][1] * nx + nabar[f][2] * ny;
-        abar[0] += nabar[f][0];
-        abar[1] += nabar[f][1] - R(2) * dm * nx;
-        abar[2] += nabar[f][2] - R(2) * dm * ny;
-        abar[3] += nabar[f][3];
-      } else if (kind == CFD_FACE_FIXED_STATE && P.bc_bar) {
-        const int row = m.neighbor[f * ld + e];
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if (nabar[f][c] != R(0)) atomicAdd(&P.bc_bar[row * 4 + c], (double)nabar[f][c]);
+        const R n1 = __shfl_sync(qmask, nabar[f], base + 1), n2 = __shfl_sync(qmask, nabar[f], base + 2);
+        const R dm = n1 * nx + n2 * ny;
+        abar += c == 1 ? nabar[f] - R(2) * dm * nx : (c == 2 ? nabar[f] - R(2) * dm * ny : nabar[f]);
+      } else if (kind >= CFD_FACE_FIXED_STATE && P.bc_bar) {  // fixed or exact state: its ghost row
+        const int row = m.neighbor[f * ld + e] + (kind == CFD_FACE_EXACT_STATE ? NFP : 0);
+        if (nabar[f] != R(0)) atomicAdd(&P.bc_bar[row * 4 + c], (double)nabar[f]);
       }
-      if (kind != CFD_FACE_INTERIOR) nabar[f][0] = nabar[f][1] = nabar[f][2] = nabar[f][3] = R(0);
+      if (kind != CFD_FACE_INTERIOR) nabar[f] = R(0);
     }
   }
 #pragma unroll
-  for (int i = 0; i < NP; ++i)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) qtb[(c * NP + i) * ld + e] = y[i][c] + (R)tab::AVG_W[i] * abar[c];
+  for (int i = 0; i < NP; ++i) qtb[(c * NP + i) * ld + e] = y[i] + (R)tab::AVG_W[i] * abar;
   if (PHI != LIM_UNLIMITED) {
 #pragma unroll
-    for (int f = 0; f < 3; ++f)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) nab[(f * 4 + c) * ld + e] = nabar[f][c];
+    for (int f = 0; f < 3; ++f) nab[(f * 4 + c) * ld + e] = nabar[f];
   }
 }
 
-// the listed elements, grid-stride
+// the listed elements, grid-stride, four lanes per element
 template <typename R, int PHI>
 __global__ void __launch_bounds__(64) adj_limit_heavy_kernel(const AdjParams P) {
   const int n = *P.count;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-    adj_limit_element<R, PHI>(P, P.list[t]);
+  const int lane = threadIdx.x & 31, c = lane & 3, base = lane & ~3;
+  const unsigned qmask = 0xfu << base;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < n; t += (gridDim.x * blockDim.x) >> 2)
+    adj_limit_quad<R, PHI>(P, P.list[t], c, qmask, base);
 }
 
 // surface pass A: w = b dt Fscale LIFT^T qt_bar at the 15 face nodes; one
@@ -590,22 +581,29 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const AdjParams P) {
   R fs[3];
 #pragma unroll
   for (int f = 0; f < 3; ++f) fs[f] = scale * (R)m.face_geo[(3 * f + 2) * ld + e];
+  const bool own = P.listed[e] != 0;
+  const R* __restrict__ src = own ? v : (const R*)P.g;
   R vi[NP];
 #pragma unroll
-  for (int i = 0; i < NP; ++i) vi[i] = v[(c * NP + i) * ld + e];
+  for (int i = 0; i < NP; ++i) vi[i] = src[(c * NP + i) * ld + e];
   if (P.limited) {
-    // the neighbours' adjoints of this element's average (they read it in
-    // their troubled-cell tests): qt_bar += AVG_W * sum, written back for
-    // the node pass
+    // the listed neighbours' adjoints of this element's average (they read
+    // it in their troubled-cell tests): qt_bar += AVG_W * sum, written to
+    // qtb for the node pass whenever a neighbour is listed (adj_uses_qtb)
     const int finfo = m.face_info[e];
     const R* __restrict__ nab = (const R*)P.nab;
     R ab = R(0);
+    bool nb_listed = false;
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       const int info = (finfo >> (8 * f)) & 0xff;
-      if ((info & 3) == CFD_FACE_INTERIOR) ab += nab[(((info >> 2) & 3) * 4 + c) * ld + m.neighbor[f * ld + e]];
+      if ((info & 3) != CFD_FACE_INTERIOR) continue;
+      const int nb = m.neighbor[f * ld + e];
+      if (!P.listed[nb]) continue;
+      nb_listed = true;
+      ab += nab[(((info >> 2) & 3) * 4 + c) * ld + nb];
     }
-    if (ab != R(0)) {
+    if (nb_listed) {
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
         vi[i] += (R)tab::AVG_W[i] * ab;
@@ -630,18 +628,19 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const AdjParams P) {
 // at node j: the volume term at j and the surface terms of the face slots
 // that meet at j (corner nodes lie on two faces).
 constexpr int ADJ_EPB = 32;
+constexpr int ADJ_NODE_MINB = 1;  // resident blocks per SM the register budget is sized for
 
 template <typename R, int FLUX>
-__global__ void __launch_bounds__(ADJ_EPB * NP) adj_rhs_node_kernel(const AdjParams P) {
+__global__ void __launch_bounds__(ADJ_EPB * NP, ADJ_NODE_MINB) adj_rhs_node_kernel(const AdjParams P) {
   __shared__ R s_v[4 * NP][ADJ_EPB];
   const CfdMesh& m = P.m;
   const int ld = m.ld;
   const int lane = threadIdx.x, j = threadIdx.y;
   const int e = blockIdx.x * ADJ_EPB + lane;
   const bool in = e < m.num_elements;
-  const R* __restrict__ qtb = (const R*)P.qtb;
+  const R* __restrict__ vsrc = (const R*)(in && adj_uses_qtb(P, e) ? P.qtb : P.g);
 #pragma unroll
-  for (int r = j; r < 4 * NP; r += NP) s_v[r][lane] = in ? qtb[r * ld + e] : R(0);
+  for (int r = j; r < 4 * NP; r += NP) s_v[r][lane] = in ? vsrc[r * ld + e] : R(0);
   __syncthreads();
   if (!in) return;
   const int inst = element_instance(m, e);
@@ -725,7 +724,7 @@ __global__ void __launch_bounds__(ADJ_EPB * NP) adj_rhs_node_kernel(const AdjPar
       acc[2] += jfm[2] - jm[2] - (jp[2] - R(2) * dm * ny);
       acc[3] += jfm[3] - jm[3] - jp[3];
     } else {
-      const int row = m.neighbor[f * ld + e];
+      const int row = m.neighbor[f * ld + e] + (kind == CFD_FACE_EXACT_STATE ? k : 0);
 #pragma unroll
       for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
       R jm[4];

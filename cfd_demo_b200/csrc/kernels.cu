@@ -681,16 +681,20 @@ double* tape_aux(void* tape, int ld, int precision, int k) { return tape_avg(tap
 double* tape_pos(void* tape, int ld, int precision, int k) { return tape_avg(tape, ld, precision, k) + (size_t)7 * ld; }
 // adjoint scratch: qt_bar, face-node adjoints w, neighbour-average adjoints,
 // the adjoints of q1 and q2 (60 + 60 + 12 + 60 + 60 rows of the solver
-// precision), the list of elements for the full limiter replay (ld ints) and
-// its counter
+// precision), the list of elements for the full limiter replay (ld ints), its
+// counter (in a 256-byte slot) and the per-element listed flags (ld bytes)
 size_t adjoint_reals_bytes(int ld, int precision) { return (size_t)252 * ld * (precision == CFD_FP64 ? 8 : 4); }
-size_t adjoint_work_bytes(int ld, int precision) { return adjoint_reals_bytes(ld, precision) + (size_t)4 * ld + 256; }
+size_t adjoint_work_bytes(int ld, int precision) {
+  return adjoint_reals_bytes(ld, precision) + (size_t)4 * ld + 256 + (((size_t)ld + 255) & ~(size_t)255);
+}
 
 template <typename R, int PHI>
 void launch_adj_limit_phi(const AdjParams& p, int n, cudaStream_t st) {
   adj_limit_scan_kernel<R, PHI><<<blocks_for(n, 128), 128, 0, st>>>(p);
-  // the listed elements are a small minority: a grid of a few blocks per SM
-  const unsigned hb = (unsigned)(blocks_for(n, 64) < 4 * 148 ? blocks_for(n, 64) : 4 * 148);
+  // four lanes per listed element; the list's length is only known on the
+  // device, so the grid covers up to 37,888 elements per sweep (16 blocks of
+  // 64 threads per SM) and strides over the rest
+  const unsigned want = blocks_for(4LL * n, 64), hb = want < 16 * 148 ? want : 16 * 148;
   adj_limit_heavy_kernel<R, PHI><<<hb, 64, 0, st>>>(p);
 }
 template <typename R>
@@ -800,6 +804,7 @@ int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape,
   void* b2 = (char*)b1 + sb;                      // adjoint of q2
   int* list = (int*)(wk + adjoint_reals_bytes(ld, prec));
   int* count = (int*)(wk + adjoint_reals_bytes(ld, prec) + (size_t)4 * ld);
+  uint8_t* listed = (uint8_t*)(wk + adjoint_reals_bytes(ld, prec) + (size_t)4 * ld + 256);
   void* tp = const_cast<void*>(tape);
   if (cudaMemsetAsync(g_in, 0, sb, st) != cudaSuccess) return check_launch("cfd_rk3_step_adjoint: memset");
   const int n = s->mesh.num_elements;
@@ -829,6 +834,7 @@ int cfd_rk3_step_adjoint(const CfdSolver* s, const void* q_in, const void* tape,
     p.hold_theta = (flags & CFD_ADJ_HOLD_THETA) != 0;
     p.list = list;
     p.count = count;
+    p.listed = listed;
     if (cudaMemsetAsync(count, 0, sizeof(int), st) != cudaSuccess) return check_launch("cfd_rk3_step_adjoint: memset");
     if (prec == CFD_FP64) {
       launch_adj_limit<double>(p, s->limiter, n, st);

@@ -73,7 +73,8 @@ __device__ __forceinline__ void limit_body(const LimitParams& P, int e, int par,
           na[2] = xsub(a[2], xmul(xmul(2.0, mn), ny));
           na[3] = a[3];
         } else {
-          const int row = m.neighbor[f * ld + e];
+          // the ghost average: the fixed state, or the exact state's row after its node rows
+          const int row = m.neighbor[f * ld + e] + (kind == CFD_FACE_EXACT_STATE ? NFP : 0);
 #pragma unroll
           for (int c = 0; c < 4; ++c) na[c] = m.bc_states[row * 4 + c];
         }

@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(BS, (sizeof(R) == 4 ? 512 : 384) / BS) stage_p
         const int kind = info & 3;
         const int nf = (info >> 2) & 3;
         const R nx = fg[(3 * f) * ld + e], ny = fg[(3 * f + 1) * ld + e], fs = fg[(3 * f + 2) * ld + e];
-        const int nb = (kind != CFD_FACE_SLIP_WALL) ? m.neighbor[f * ld + e] : 0;
+        // interior: the neighbour; fixed state: the face's row; exact state: the node's row
+        const int nb = (kind != CFD_FACE_SLIP_WALL) ? m.neighbor[f * ld + e] + (kind == CFD_FACE_EXACT_STATE ? k : 0) : 0;
         const double bw = (kind != CFD_FACE_INTERIOR) ? ctab::FACE_W[k] * m.face_hlen[f * ld + e] : 0.0;
         const bool same_order = (f == 2) != (nf == 2);
         const int pn = face_node_rt(nf, same_order ? k : NFP - 1 - k);

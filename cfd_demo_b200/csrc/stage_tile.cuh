@@ -448,7 +448,8 @@ __device__ __forceinline__ void stage_tile_body(const StageParams& P, const int 
           qp[2] = qm[2] - R(2) * mn * ny;
           qp[3] = qm[3];
         } else {
-          const int row = t_int[(1 + f) * EPB + os];
+          // fixed state: one row per face; exact state: one row per face node
+          const int row = t_int[(1 + f) * EPB + os] + (kind == CFD_FACE_EXACT_STATE ? k : 0);
 #pragma unroll
           for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
         }
@@ -510,7 +511,8 @@ __device__ __forceinline__ void stage_tile_body(const StageParams& P, const int 
           qp[2] = qm[2] - R(2) * mn * ny;
           qp[3] = qm[3];
         } else {
-          const int row = t_int[(1 + f) * EPB + slot];
+          // fixed state: one row per face; exact state: one row per face node
+          const int row = t_int[(1 + f) * EPB + slot] + (kind == CFD_FACE_EXACT_STATE ? k : 0);
 #pragma unroll
           for (int c = 0; c < 4; ++c) qp[c] = (R)m.bc_states[row * 4 + c];
         }

@@ -102,6 +102,25 @@ def jittered_rectangle_mesh(nx: int, ny: int, amplitude: float, seed: int,
     return TriangleMesh(vertices=v, elements=m.elements, boundary_edges=m.boundary_edges)
 
 
+def sheared_rectangle_mesh(nx: int, ny: int, slope_angle: float, x_range=(0.0, 1.0),
+                           y_range=(0.0, 1.0)) -> TriangleMesh:
+    """rectangle_mesh mapped by (x, y) -> (x, y + x tan(slope_angle)), the
+    affine shear of CFD-demo's proposed ADR 0012 (docs/adr/0012-...:22-31):
+    vertices only, so the elements, the lower-left to upper-right diagonal
+    and the tags are those of the rectangle; `bottom` becomes the inclined
+    wall y = x tan(slope_angle) + y0 and `top` the sheared upper boundary.
+    slope_angle in radians, |slope_angle| < pi/2; zero gives rectangle_mesh
+    exactly."""
+    if not abs(slope_angle) < 0.5 * np.pi:
+        raise ValueError("slope_angle must lie strictly between -pi/2 and pi/2.")
+    m = rectangle_mesh(nx, ny, x_range, y_range)
+    if slope_angle == 0.0:
+        return m
+    v = np.array(m.vertices)
+    v[:, 1] = v[:, 1] + v[:, 0] * np.tan(slope_angle)
+    return TriangleMesh(vertices=v, elements=m.elements, boundary_edges=m.boundary_edges)
+
+
 @dataclass(frozen=True, eq=False)
 class MeshConnectivity:
     """Face connectivity (mesh.py:115-132): neighbour element / local face per

@@ -14,7 +14,8 @@ leading dimension ``ld`` so that a warp's loads of one field are contiguous:
     neighbor   [3][ld]  neighbour element, or fixed-state row   int32
     face_info  [ld]     per face 8 bits: kind | nbr face << 2 | partner face << 4
     instance   [ld]     instance id (batched meshes only)       int32
-    bc_states  [rows][4] fixed exterior states                 float64
+    bc_states  [rows][4] fixed exterior states; per exact-state face 6 rows (its 5
+                         face-node states, then its ghost average)  float64
 
 Several meshes ("instances") can be concatenated into one table set; element
 and neighbour indices are then global.
@@ -28,7 +29,7 @@ from typing import NamedTuple
 import numpy as np
 
 from . import _native
-from .boundary import FIXED_STATE, SLIP_WALL
+from .boundary import EXACT_STATE, FIXED_STATE, SLIP_WALL
 from .mesh import MeshConnectivity, TriangleMesh, element_geometry, node_coordinates
 
 COEFFICIENT_TOLERANCE = 1e-12  # limiting.py:31
@@ -56,9 +57,74 @@ def resolve_boundary_conditions(connectivity: MeshConnectivity, boundary_conditi
         kind[mask] = bc.kind
         if bc.kind == FIXED_STATE:
             state[mask] = bc.state
-        elif bc.kind != SLIP_WALL:
+        elif bc.kind not in (SLIP_WALL, EXACT_STATE):
             raise ValueError(f"Unsupported boundary condition for tag {tag!r}: {bc!r}.")
     return kind, state
+
+
+def reflected_triangles(mesh: TriangleMesh, elements: np.ndarray, faces: np.ndarray) -> np.ndarray:
+    """The corners (n, 3, 2) of each listed element reflected across the line
+    of its listed face (local face f joins local vertices f and f+1)."""
+    c = mesh.vertices[mesh.elements[elements]]  # (n, 3, 2)
+    a = c[np.arange(len(faces)), faces]
+    b = c[np.arange(len(faces)), (faces + 1) % 3]
+    d = b - a
+    nrm = np.stack([d[:, 1], -d[:, 0]], axis=-1) / np.linalg.norm(d, axis=-1, keepdims=True)
+    off = np.einsum("nvd,nd->nv", c - a[:, None], nrm)
+    return c - 2.0 * off[..., None] * nrm[:, None]
+
+
+def sampled_cell_average(bc, corners: np.ndarray, subdivisions: int = 32) -> np.ndarray:
+    """Cell averages (n, 4) of bc.states over triangles (n, 3, 2): the mean of
+    the values at the centroids of the subdivisions**2 equal sub-triangles."""
+    m = subdivisions
+    i, j = np.meshgrid(np.arange(m), np.arange(m), indexing="ij")
+    up = (i + j) < m
+    b_up = np.stack([(i + 1 / 3), (j + 1 / 3)], axis=-1)[up] / m
+    dn = (i + j) < m - 1
+    b_dn = np.stack([(i + 2 / 3), (j + 2 / 3)], axis=-1)[dn] / m
+    lam = np.concatenate([b_up, b_dn])  # barycentric weights of corners 1 and 2
+    w = np.stack([1.0 - lam[:, 0] - lam[:, 1], lam[:, 0], lam[:, 1]], axis=-1)  # (m^2, 3)
+    pts = np.einsum("pv,nvd->npd", w, corners)
+    return bc.states(pts[..., 0], pts[..., 1]).mean(axis=1)
+
+
+@dataclass
+class ExactRows:
+    """Exterior-state rows of the exact-state faces, face by face in (element,
+    face) order: the states at the face's nodes (element face-node order) and
+    the ghost average across it."""
+
+    elements: np.ndarray  # (n,)
+    faces: np.ndarray  # (n,)
+    node_states: np.ndarray  # (n, Nfp, 4)
+    ghost: np.ndarray  # (n, 4)
+
+
+def exact_state_rows(mesh: TriangleMesh, connectivity: MeshConnectivity, reference, kind: np.ndarray,
+                     boundary_conditions) -> ExactRows:
+    """Evaluate every ExactState boundary condition once: at the face nodes of
+    its faces (the interface flux's exterior states) and, as the ghost
+    average, over each boundary element reflected across the face (the
+    condition's own cell_average(corners) when it has one, else a sampled
+    average)."""
+    e_idx, f_idx = np.nonzero(kind == EXACT_STATE)
+    nfp = reference.face_nodes.shape[1]
+    node_states = np.zeros((len(e_idx), nfp, 4))
+    ghost = np.zeros((len(e_idx), 4))
+    if len(e_idx):
+        x, y = node_coordinates(mesh, reference.r, reference.s)
+        fn = np.asarray(reference.face_nodes)[f_idx]  # (n, Nfp) node ids
+        fx, fy = x[fn, e_idx[:, None]], y[fn, e_idx[:, None]]
+        corners = reflected_triangles(mesh, e_idx, f_idx)
+        tags = connectivity.face_tag[e_idx, f_idx]
+        for ti in np.unique(tags):
+            sel = tags == ti
+            bc = boundary_conditions[connectivity.boundary_tags[ti]]
+            node_states[sel] = bc.states(fx[sel], fy[sel])
+            average = getattr(bc, "cell_average", None)
+            ghost[sel] = average(corners[sel]) if average is not None else sampled_cell_average(bc, corners[sel])
+    return ExactRows(e_idx, f_idx, node_states, ghost)
 
 
 def neighbor_coefficients(connectivity: MeshConnectivity, geometry) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
@@ -192,7 +258,9 @@ class HostTables:
 
 
 def host_tables(mesh: TriangleMesh, connectivity: MeshConnectivity, geometry, reference, kind: np.ndarray,
-                state: np.ndarray, degree: int = 4, device=None) -> HostTables:
+                state: np.ndarray, degree: int = 4, device=None, boundary_conditions=None) -> HostTables:
+    """One mesh's tables. Exact-state faces (kind EXACT_STATE) need the
+    boundary conditions to evaluate their rows."""
     k = mesh.num_elements
     check_face_pairing(mesh, connectivity, reference, geometry=geometry, device=device)
     alpha, beta, partner = neighbor_coefficients(connectivity, geometry)
@@ -200,8 +268,17 @@ def host_tables(mesh: TriangleMesh, connectivity: MeshConnectivity, geometry, re
     fixed = kind == FIXED_STATE
     rows, inverse = (np.unique(state[fixed], axis=0, return_inverse=True) if fixed.any()
                      else (np.zeros((0, 4)), np.zeros(0, dtype=np.int64)))
+    rows = np.asarray(rows, dtype=np.float64).reshape(-1, 4)
     nbr = np.where(connectivity.neighbor_element >= 0, connectivity.neighbor_element, 0).astype(np.int64)
     nbr[fixed] = inverse.reshape(-1)
+    if (kind == EXACT_STATE).any():
+        if boundary_conditions is None:
+            raise ValueError("Exact-state faces need the boundary conditions to build their rows.")
+        ex = exact_state_rows(mesh, connectivity, reference, kind, boundary_conditions)
+        nfp = ex.node_states.shape[1]
+        blocks = np.concatenate([ex.node_states, ex.ghost[:, None]], axis=1).reshape(-1, 4)  # (n (Nfp+1), 4)
+        nbr[ex.elements, ex.faces] = len(rows) + (nfp + 1) * np.arange(len(ex.elements))
+        rows = np.concatenate([rows, blocks])
     nface = np.where(connectivity.neighbor_face >= 0, connectivity.neighbor_face, 0)
     info = np.zeros(k, dtype=np.int64)
     for f in range(3):
@@ -224,7 +301,7 @@ def host_tables(mesh: TriangleMesh, connectivity: MeshConnectivity, geometry, re
         cs_coef=np.concatenate([alpha.T, beta.T]),
         neighbor=nbr.T.astype(np.int32),
         face_info=info.astype(np.int32),
-        bc_states=np.asarray(rows, dtype=np.float64).reshape(-1, 4),
+        bc_states=rows,
         interior=(connectivity.neighbor_element >= 0).T,
     )
 
@@ -296,7 +373,7 @@ class DeviceTables:
         for i, (p, o) in enumerate(zip(parts, self.offsets[:-1])):
             kinds = np.stack([(p.face_info >> (8 * f)) & 3 for f in range(3)])
             local = p.neighbor.astype(np.int64)
-            glob = np.where(kinds == FIXED_STATE, local + bc_off[i], np.where(kinds == 0, local + o, 0))
+            glob = np.where(kinds >= FIXED_STATE, local + bc_off[i], np.where(kinds == 0, local + o, 0))
             nbr[:, o:o + p.num_elements] = glob
             info[o:o + p.num_elements] = p.face_info
             inst[o:o + p.num_elements] = i
@@ -341,11 +418,22 @@ class DeviceTables:
         """One mesh's tables built by the GPU (cfd_mesh_build): geometry,
         connectivity and boundary tags, Cockburn-Shu coefficients and the
         face-node pairing check, bit for bit the host builder's tables. An
-        invalid mesh is reported with the host builder's error."""
+        invalid mesh is reported with the host builder's error. Exact-state
+        boundaries (per-node rows evaluated by a Python function) take the
+        host builder."""
         import ctypes as C
 
         import torch
 
+        if any(getattr(bc, "kind", None) == EXACT_STATE for bc in boundary_conditions.values()):
+            from .mesh import build_connectivity
+
+            conn = build_connectivity(mesh)
+            geo = element_geometry(mesh)
+            kind, state = resolve_boundary_conditions(conn, boundary_conditions)
+            part = host_tables(mesh, conn, geo, reference, kind, state, device=device,
+                               boundary_conditions=boundary_conditions)
+            return cls([part], device, precision)
         tags, kinds, tag_row, rows = boundary_tag_tables(mesh, boundary_conditions)
         dev = torch.device(device)
         k = mesh.num_elements

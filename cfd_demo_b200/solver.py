@@ -25,12 +25,13 @@ from typing import NamedTuple
 import numpy as np
 
 from . import _native
-from .boundary import BoundaryCondition
+from .boundary import EXACT_STATE, BoundaryCondition
 from .euler import NUM_VARIABLES
 from .fluxes import FLUX_IDS, get_interface_flux
 from .limiters import LIMITER_IDS, get_limiter_function
 from .mesh import TriangleMesh, build_connectivity, element_geometry, node_coordinates
-from .operators import DeviceTables, LimiterOperators, limiter_operators, resolve_boundary_conditions
+from .operators import (DeviceTables, LimiterOperators, exact_state_rows, limiter_operators,
+                        resolve_boundary_conditions)
 from .reference_element import DEGREE, build_reference_triangle
 
 DEFAULT_CFL = 0.5  # time_integration.py:18
@@ -246,6 +247,10 @@ class EulerSolver:
         ops = getattr(self, "_limiter_operators", None)
         if ops is None:
             kind, state = resolve_boundary_conditions(self.connectivity, self.boundary_conditions)
+            if (kind == EXACT_STATE).any():  # the ghost averages stand in for the exterior state
+                ex = exact_state_rows(self.mesh, self.connectivity, self.reference, kind, self.boundary_conditions)
+                state = state.copy()
+                state[ex.elements, ex.faces] = ex.ghost
             ops = limiter_operators(self.connectivity, self.geometry, self.reference, kind, state)
             self._limiter_operators = ops
         return ops

@@ -15,6 +15,12 @@ with PyTorch on the GPU.
 * ``l1_errors``, ``column_density`` / ``front_position``: the domain-averaged
   L1 errors against the exact solution and the discontinuity positions taken
   from the mesh-column averages of the density.
+* ``ObliqueShock``: the steady attached oblique shock of a uniform supersonic
+  stream turned by a wedge (the theta-beta-M relation, weak branch, and the
+  normal-shock jumps; Anderson, "Modern Compressible Flow", ch. 4), the
+  exact solution of CFD-demo's proposed ADR 0011 verification case, with
+  exact cell averages over triangles; ``oblique_l1_errors`` and
+  ``shock_angle_at`` are its diagnostics.
 
 These are the diagnostics CFD-demo's verification tests compute with NumPy
 (tests/verification/diagnostics.py, sod_reference.py, ADR 0005 checks); here
@@ -170,6 +176,22 @@ def collapsed_gauss(n: int = 10) -> tuple[np.ndarray, np.ndarray]:
     return np.stack([1.0 - l1 - l2, l1, l2], axis=-1), weight
 
 
+def _clip_line(poly: np.ndarray, normal, c: float, keep_above: bool) -> np.ndarray:
+    """Convex polygon clipped to n . p >= c (keep_above) or n . p <= c."""
+    d = poly @ np.asarray(normal, dtype=np.float64) - c
+    if not keep_above:
+        d = -d
+    out = []
+    n = len(poly)
+    for i in range(n):
+        j = (i + 1) % n
+        if d[i] >= 0.0:
+            out.append(poly[i])
+        if (d[i] >= 0.0) != (d[j] >= 0.0):
+            out.append(poly[i] + d[i] / (d[i] - d[j]) * (poly[j] - poly[i]))
+    return np.array(out).reshape(-1, 2)
+
+
 def _clip(poly: np.ndarray, x: float, keep_right: bool) -> np.ndarray:
     """Convex polygon clipped to x' >= x (keep_right) or x' <= x."""
     d = (poly[:, 0] - x) if keep_right else (x - poly[:, 0])
@@ -205,16 +227,22 @@ class Quadrature:
         return float(self.weight.sum())
 
 
-def quadrature(mesh, breaks=(), n: int = 10, tol: float = 1e-12) -> Quadrature:
+def quadrature(mesh, breaks=(), n: int = 10, tol: float = 1e-12, lines=()) -> Quadrature:
     """Integration points over the mesh; elements crossed by a vertical line
-    x = b (b in ``breaks``) are cut along it and fan-triangulated."""
+    x = b (b in ``breaks``) or by a line n . p = c ((nx, ny, c) in ``lines``,
+    n a unit normal) are cut along it and fan-triangulated."""
     corners = mesh.vertices[mesh.elements]  # (K, 3, 2)
     bary, w = collapsed_gauss(n)
     breaks = np.sort(np.asarray(breaks, dtype=np.float64).reshape(-1))
     xmin, xmax = corners[..., 0].min(1), corners[..., 0].max(1)
     span = np.maximum(xmax - xmin, tol)
     cut = (breaks[None, :] > (xmin + tol * span)[:, None]) & (breaks[None, :] < (xmax - tol * span)[:, None])
-    split = np.flatnonzero(cut.any(1))
+    lines = [tuple(float(v) for v in ln) for ln in lines]
+    line_cut = np.zeros((len(corners), len(lines)), dtype=bool)
+    for li, (lnx, lny, lc) in enumerate(lines):
+        d = corners[..., 0] * lnx + corners[..., 1] * lny - lc
+        line_cut[:, li] = (d.max(1) > tol * span) & (d.min(1) < -tol * span)
+    split = np.flatnonzero(cut.any(1) | line_cut.any(1))
     whole = np.setdiff1d(np.arange(len(corners)), split)
     # reference coordinates of the rule's points in the reference triangle (-1,-1), (1,-1), (-1,1)
     ref_r = -bary[:, 0] + bary[:, 1] - bary[:, 2]
@@ -228,12 +256,19 @@ def quadrature(mesh, breaks=(), n: int = 10, tol: float = 1e-12) -> Quadrature:
     for e in split:
         edges = np.concatenate(([-np.inf], breaks[cut[e]], [np.inf]))
         tri = corners[e]
+        slabs = []
         for lo, hi in zip(edges[:-1], edges[1:]):
             piece = tri
             if np.isfinite(lo):
                 piece = _clip(piece, lo, keep_right=True)
             if len(piece) >= 3 and np.isfinite(hi):
                 piece = _clip(piece, hi, keep_right=False)
+            slabs.append(piece)
+        for li in np.flatnonzero(line_cut[e]):
+            lnx, lny, lc = lines[li]
+            slabs = [h for p in slabs if len(p) >= 3
+                     for h in (_clip_line(p, (lnx, lny), lc, True), _clip_line(p, (lnx, lny), lc, False))]
+        for piece in slabs:
             for k in range(1, len(piece) - 1):
                 sub = np.stack([piece[0], piece[k], piece[k + 1]])
                 a2 = abs((sub[1, 0] - sub[0, 0]) * (sub[2, 1] - sub[0, 1]) - (sub[1, 1] - sub[0, 1]) * (sub[2, 0] - sub[0, 0]))
@@ -328,3 +363,188 @@ def front_position(column_avg: np.ndarray, face_x: np.ndarray, window) -> float:
         raise ValueError(f"No column face lies in {window}.")
     drop = np.where(inside, column_avg[:-1] - column_avg[1:], -np.inf)
     return float(face_x[int(np.argmax(drop))])
+
+
+# ------------------------------------------------------ oblique shock (ADR 0011) ---
+class ObliqueShock:
+    """The steady oblique shock of CFD-demo's proposed verification case
+    (docs/adr/0011-oblique-shock-verification.md:31-45): the upstream state
+    (rho, u, v, p) = (1, M1, 0, 1/gamma) (sound speed 1) turned by a wall of
+    slope angle theta through the attached weak shock y = x tan(beta) from the
+    corner at the origin. Below the shock (between it and the wall) the
+    post-shock state is uniform and moves parallel to the wall.
+
+    beta solves the theta-beta-M relation
+        tan(theta) = 2 cot(beta) (M1^2 sin^2 beta - 1) / (M1^2 (gamma + cos 2 beta) + 2)
+    on its weak branch (between the Mach angle asin(1/M1) and the angle of
+    maximum deflection); the post-shock state follows from the normal-shock
+    jumps at the normal Mach number M1 sin(beta). Only 0 < theta < theta_max(M1)
+    is accepted."""
+
+    def __init__(self, mach: float, wall_angle: float, gamma: float = 1.4):
+        mach, theta, gamma = float(mach), float(wall_angle), float(gamma)
+        if not mach > 1.0:
+            raise ValueError("The inflow Mach number must exceed 1.")
+        theta_max, beta_max = self.max_deflection(mach, gamma)
+        if not 0.0 < theta < theta_max:
+            raise ValueError(f"The wall angle must lie in (0, {math.degrees(theta_max):.6f} deg) for an attached "
+                             f"shock at Mach {mach}; got {math.degrees(theta):.6f} deg.")
+        self.mach, self.theta, self.gamma = mach, theta, gamma
+        self.theta_max, self.beta_max = theta_max, beta_max
+        lo, hi = math.asin(1.0 / mach), beta_max
+        for _ in range(200):  # theta(beta) increases on the weak branch
+            mid = 0.5 * (lo + hi)
+            if self.deflection(mach, mid, gamma) < theta:
+                lo = mid
+            else:
+                hi = mid
+            if hi - lo < 1e-16:
+                break
+        self.beta = 0.5 * (lo + hi)
+        g = gamma
+        self.upstream = (1.0, mach, 0.0, 1.0 / g)
+        mn1 = mach * math.sin(self.beta)
+        rho2 = (g + 1.0) * mn1 * mn1 / ((g - 1.0) * mn1 * mn1 + 2.0)
+        p2 = (1.0 + 2.0 * g / (g + 1.0) * (mn1 * mn1 - 1.0)) / g
+        mn2 = math.sqrt((1.0 + 0.5 * (g - 1.0) * mn1 * mn1) / (g * mn1 * mn1 - 0.5 * (g - 1.0)))
+        m2 = mn2 / math.sin(self.beta - theta)
+        speed = m2 * math.sqrt(g * p2 / rho2)
+        self.downstream = (rho2, speed * math.cos(theta), speed * math.sin(theta), p2)
+        self.downstream_mach = m2
+
+    @staticmethod
+    def deflection(mach: float, beta: float, gamma: float = 1.4) -> float:
+        """theta(beta) of the theta-beta-M relation."""
+        num = 2.0 / math.tan(beta) * (mach * mach * math.sin(beta) ** 2 - 1.0)
+        den = mach * mach * (gamma + math.cos(2.0 * beta)) + 2.0
+        return math.atan(num / den)
+
+    @classmethod
+    def max_deflection(cls, mach: float, gamma: float = 1.4) -> tuple[float, float]:
+        """(theta_max, beta at theta_max) by golden-section search: theta(beta)
+        is unimodal between the Mach angle and pi/2."""
+        a, b = math.asin(1.0 / mach), 0.5 * math.pi
+        r = 0.5 * (math.sqrt(5.0) - 1.0)
+        c, d = b - r * (b - a), a + r * (b - a)
+        fc, fd = cls.deflection(mach, c, gamma), cls.deflection(mach, d, gamma)
+        for _ in range(200):
+            if fc > fd:
+                b, d, fd = d, c, fc
+                c = b - r * (b - a)
+                fc = cls.deflection(mach, c, gamma)
+            else:
+                a, c, fc = c, d, fd
+                d = a + r * (b - a)
+                fd = cls.deflection(mach, d, gamma)
+            if b - a < 1e-15:
+                break
+        beta = 0.5 * (a + b)
+        return cls.deflection(mach, beta, gamma), beta
+
+    def _conserved(self, prim) -> np.ndarray:
+        rho, u, v, p = prim
+        return np.array([rho, rho * u, rho * v, p / (self.gamma - 1.0) + 0.5 * rho * (u * u + v * v)])
+
+    def below_shock(self, x, y):
+        """True in the post-shock region: downstream of the corner and below
+        the shock line."""
+        x, y = np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)
+        return (x > 0.0) & (y < x * math.tan(self.beta))
+
+    def primitive(self, x, y):
+        """(rho, u, v, p) arrays of the exact solution at (x, y)."""
+        below = self.below_shock(x, y)
+        return tuple(np.where(below, d, u_) for u_, d in zip(self.upstream, self.downstream))
+
+    def conserved(self, x, y) -> np.ndarray:
+        """Conserved states, shape x.shape + (4,)."""
+        below = self.below_shock(x, y)[..., None]
+        return np.where(below, self._conserved(self.downstream), self._conserved(self.upstream))
+
+    def cell_average(self, corners: np.ndarray) -> np.ndarray:
+        """Exact cell averages (n, 4) over triangles (n, 3, 2): the area of
+        each triangle below the shock line (and right of the corner) from
+        exact polygon clipping."""
+        corners = np.asarray(corners, dtype=np.float64)
+        nb = np.array([math.sin(self.beta), -math.cos(self.beta)])  # n . p > 0 below the line
+        down, up = self._conserved(self.downstream), self._conserved(self.upstream)
+        out = np.empty((len(corners), 4))
+        for i, tri in enumerate(corners):
+            area = 0.5 * abs((tri[1, 0] - tri[0, 0]) * (tri[2, 1] - tri[0, 1])
+                             - (tri[1, 1] - tri[0, 1]) * (tri[2, 0] - tri[0, 0]))
+            piece = _clip_line(tri, nb, 0.0, True)
+            if len(piece) >= 3:
+                piece = _clip_line(piece, (1.0, 0.0), 0.0, True)
+            below = 0.0
+            for k in range(1, len(piece) - 1):
+                a, b, c = piece[0], piece[k], piece[k + 1]
+                below += 0.5 * abs((b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0]))
+            f = min(max(below / area, 0.0), 1.0)
+            out[i] = f * down + (1.0 - f) * up
+        return out
+
+    def shock_line(self) -> tuple[float, float, float]:
+        """(nx, ny, c) of the shock line n . p = c (unit normal)."""
+        return (math.sin(self.beta), -math.cos(self.beta), 0.0)
+
+
+def oblique_l1_errors(q, mesh, exact: ObliqueShock, gamma: float, n: int = 10, region=None) -> dict:
+    """Domain-averaged L1 errors of density, pressure and both velocity
+    components against the exact oblique-shock solution, elements cut along
+    the shock line. ``region(x, y)`` (a boolean mask function) restricts the
+    integral, e.g. to the post-shock region."""
+    import torch
+
+    quad = quadrature(mesh, (), n, lines=[exact.shock_line()])
+    vals = evaluate(q, quad)
+    rho, u, v, p = primitive(vals, gamma)
+    keep = np.ones(len(quad.x), dtype=bool) if region is None else np.asarray(region(quad.x, quad.y), dtype=bool)
+    w = torch.as_tensor(np.where(keep, quad.weight, 0.0), device=q.device, dtype=q.dtype)
+    ex = [torch.as_tensor(a, device=q.device, dtype=q.dtype) for a in exact.primitive(quad.x, quad.y)]
+    area = float(w.sum())
+    l1 = lambda a, b: float((w * (a - b).abs()).sum() / area)  # noqa: E731
+    return {"density": l1(rho, ex[0]), "x velocity": l1(u, ex[1]), "y velocity": l1(v, ex[2]),
+            "pressure": l1(p, ex[3]), "area": area}
+
+
+def point_values(q, mesh, x: np.ndarray, y: np.ndarray, reference=None) -> np.ndarray:
+    """The nodal solution q (Np, K, 4) at physical points (x, y) (host
+    arrays): each point is located by its barycentric coordinates in the
+    elements (brute force, in chunks); returns a (m, 4) host array."""
+    import torch
+
+    reference = reference or build_reference_triangle(DEGREE)
+    c = mesh.vertices[mesh.elements]  # (K, 3, 2)
+    p0, e1, e2 = c[:, 0], c[:, 1] - c[:, 0], c[:, 2] - c[:, 0]
+    det = e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0]
+    pts = np.stack([np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)], axis=-1)
+    parent = np.full(len(pts), -1, dtype=np.int64)
+    lam = np.zeros((len(pts), 2))
+    for s0 in range(0, len(pts), 256):
+        d = pts[s0:s0 + 256, None, :] - p0[None]
+        l1 = (d[..., 0] * e2[None, :, 1] - d[..., 1] * e2[None, :, 0]) / det[None]
+        l2 = (e1[None, :, 0] * d[..., 1] - e1[None, :, 1] * d[..., 0]) / det[None]
+        inside = (l1 >= -1e-12) & (l2 >= -1e-12) & (l1 + l2 <= 1.0 + 1e-12)
+        first = np.argmax(inside, axis=1)
+        ok = inside[np.arange(len(first)), first]
+        parent[s0:s0 + 256] = np.where(ok, first, -1)
+        lam[s0:s0 + 256, 0] = l1[np.arange(len(first)), first]
+        lam[s0:s0 + 256, 1] = l2[np.arange(len(first)), first]
+    if (parent < 0).any():
+        raise ValueError("A sample point lies outside the mesh.")
+    phi = torch.as_tensor(lagrange_at(2.0 * lam[:, 0] - 1.0, 2.0 * lam[:, 1] - 1.0, reference), device=q.device,
+                          dtype=q.dtype)
+    par = torch.as_tensor(parent, device=q.device)
+    return torch.einsum("pn,npc->pc", phi, q[:, par, :]).cpu().numpy()
+
+
+def shock_angle_at(q, mesh, exact: ObliqueShock, x: float, height: float, samples: int = 2000,
+                   reference=None) -> float:
+    """The shock angle atan(y_s / x) from the largest density drop (upwards)
+    along the vertical cut at x between the wall and the top of the domain
+    (wall at y = x tan(theta), top at y = x tan(theta) + height), in radians."""
+    y0 = x * math.tan(exact.theta)
+    ys = y0 + height * (np.arange(samples) + 0.5) / samples
+    rho = point_values(q, mesh, np.full(samples, x), ys, reference)[:, 0]
+    i = int(np.argmax(rho[:-1] - rho[1:]))
+    return math.atan(0.5 * (ys[i] + ys[i + 1]) / x)

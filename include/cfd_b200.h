@@ -65,6 +65,7 @@ extern "C" {
 #define CFD_FACE_INTERIOR 0
 #define CFD_FACE_SLIP_WALL 1
 #define CFD_FACE_FIXED_STATE 2
+#define CFD_FACE_EXACT_STATE 3
 
 /* entries of CfdSolver.limit_list ahead of its element list (counters) */
 #define CFD_LIMIT_LIST_HEADER 16
@@ -90,7 +91,11 @@ extern "C" {
  * the counterclockwise direction); the host checks this rule by coordinates.
  * neighbor[f * ld + e] is the neighbour element across face f for interior
  * faces and, for fixed-state faces, the row of bc_states (4 doubles) holding
- * the exterior state.
+ * the exterior state. For exact-state faces (CFD_FACE_EXACT_STATE: exterior
+ * states from a known solution, one per face node) it is the first of 6
+ * rows: the exterior states at the face's 5 nodes in this element's
+ * face-node order, then the ghost cell average the troubled-cell test uses
+ * across the face.
  */
 typedef struct CfdMesh {
     int32_t num_elements;  /* K: elements of all instances */

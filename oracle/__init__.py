@@ -32,8 +32,10 @@ from .mesh import (
     rectangle_mesh,
 )
 from .physics import (
+    EXACT_STATE,
     FIXED_STATE,
     SLIP_WALL,
+    ExactState,
     FixedState,
     SlipWall,
     cartesian_fluxes,
@@ -48,6 +50,8 @@ from .physics import (
 from .solver import OracleSolver, RunResult, SolverError, StepReport, sod_shock_tube
 
 __all__ = [
+    "EXACT_STATE",
+    "ExactState",
     "FIXED_STATE",
     "SLIP_WALL",
     "ElementGeometry",

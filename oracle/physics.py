@@ -15,6 +15,7 @@ import numpy as np
 
 SLIP_WALL = 1  # boundary.py:13
 FIXED_STATE = 2  # boundary.py:14
+EXACT_STATE = 3  # proposed, docs/adr/0012-sheared-rectangle-mesh-and-far-field-boundaries.md:32-46
 ROE_ENTROPY_FIX = 0.1  # fluxes.py:21
 
 
@@ -38,6 +39,20 @@ class FixedState:
     @classmethod
     def from_primitive(cls, rho, u, v, p, gamma):
         return cls((rho, rho * u, rho * v, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)))
+
+
+@dataclass(frozen=True, eq=False)
+class ExactState:
+    """The proposed far-field condition of ADR 0012 (docs/adr/0012-...:32-46),
+    not implemented in the reference: `function(x, y)` gives conserved
+    states x.shape + (4,), evaluated at the face nodes of the tagged faces;
+    the ghost average across a face is the function's cell average over the
+    boundary element reflected across that face (`cell_average(corners)`
+    when given)."""
+
+    function: object
+    cell_average: object = None
+    kind: int = EXACT_STATE
 
 
 def primitive_to_conserved(rho, u, v, p, gamma):

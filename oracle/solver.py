@@ -18,6 +18,7 @@ import numpy as np
 from .element import DEGREE, build_reference_triangle
 from .mesh import build_connectivity, element_geometry, node_coordinates, pair_face_nodes, rectangle_mesh
 from .physics import (
+    EXACT_STATE,
     FIXED_STATE,
     SLIP_WALL,
     FixedState,
@@ -121,6 +122,18 @@ class OracleSolver:
 
         # dg.py:76-116 — operator arrays in face-node layout (3 Nfp, K)
         x, y = node_coordinates(mesh, ref.r, ref.s)
+        # proposed ADR 0012: exact-state faces take per-node exterior states and
+        # the reflected element's average as the ghost average
+        node_state = np.zeros((3, nfp, k, 4))
+        for ti, tag in enumerate(conn.boundary_tags):
+            bc = boundary_conditions[tag]
+            if bc.kind != EXACT_STATE:
+                continue
+            es, fs = np.nonzero(conn.face_tag == ti)
+            for e, f in zip(es, fs):
+                nodes = ref.face_nodes[f]
+                node_state[f, :, e] = np.asarray(bc.function(x[nodes, e], y[nodes, e]), dtype=np.float64)
+                state[e, f] = self._ghost_average(bc, mesh, e, f)
         partner = pair_face_nodes(mesh, conn, x, y, ref.face_nodes)
         own = np.arange(k)[:, None]
         nbr = np.where(conn.neighbor_element >= 0, conn.neighbor_element, own)
@@ -135,7 +148,8 @@ class OracleSolver:
         self.fscale = per_node(0.5 * geo.edge_length / geo.jacobian[:, None])
         self.exterior_index = (partner * k + nbr.T[:, None, :]).reshape(3 * nfp, k)
         self.kind_fn = per_node(kind)
-        self.state_fn = per_node(state)
+        self.state_fn = np.where((self.kind_fn == EXACT_STATE)[..., None], node_state.reshape(3 * nfp, k, 4),
+                                 per_node(state))
         ew = ref.face_weights.reshape(-1)[:, None] * per_node(0.5 * geo.edge_length)
         self.bweight = np.where(self.kind_fn > 0, ew, 0.0)
         self.dmat = np.concatenate([ref.dr, ref.ds], axis=1)
@@ -152,6 +166,29 @@ class OracleSolver:
         self.dt_geometry = np.min(2.0 * geo.area[:, None] / ((ref.degree + 1) ** 2 * geo.edge_length), axis=1)
 
     # ---- setup helpers -------------------------------------------------
+    @staticmethod
+    def _ghost_average(bc, mesh, e, f, subdivisions=32):
+        """The exact-state function's average over element e reflected across
+        its face f: bc.cell_average when given, else the mean over the
+        centroids of subdivisions**2 equal sub-triangles."""
+        c = mesh.vertices[mesh.elements[e]]
+        a, b = c[f], c[(f + 1) % 3]
+        d = b - a
+        nrm = np.array([d[1], -d[0]]) / np.hypot(d[0], d[1])
+        tri = c - 2.0 * ((c - a) @ nrm)[:, None] * nrm[None]
+        if bc.cell_average is not None:
+            return np.asarray(bc.cell_average(tri[None]), dtype=np.float64)[0]
+        m = subdivisions
+        pts = []
+        for i in range(m):
+            for j in range(m - i):
+                pts.append(((i + 1 / 3) / m, (j + 1 / 3) / m))
+                if i + j < m - 1:
+                    pts.append(((i + 2 / 3) / m, (j + 2 / 3) / m))
+        lam = np.array(pts)
+        p = tri[0] + lam[:, :1] * (tri[1] - tri[0]) + lam[:, 1:] * (tri[2] - tri[0])
+        return np.asarray(bc.function(p[:, 0], p[:, 1]), dtype=np.float64).mean(axis=0)
+
     def _cs_coefficients(self):
         """limiting.py:51-94."""
         geo, conn = self.geometry, self.connectivity
@@ -206,7 +243,7 @@ class OracleSolver:
         qn = q.reshape(-1, 4)[self.exterior_index]
         kind = self.kind_fn[..., None]
         qp = np.where(kind == SLIP_WALL, mirror_state(qm, self.nx, self.ny),
-                      np.where(kind == FIXED_STATE, self.state_fn, qn))
+                      np.where(kind >= FIXED_STATE, self.state_fn, qn))
         fhat = self.flux(qm, qp, self.nx, self.ny, self.gamma)
         fminus = f[self.face_nodes] * self.nx[..., None] + g[self.face_nodes] * self.ny[..., None]
         jump = self.fscale[..., None] * (fminus - fhat)
@@ -219,7 +256,7 @@ class OracleSolver:
         interior = avg[self.nbr3]
         wall = mirror_state(avg[None], self.nx3, self.ny3)
         kind = self.kind3[..., None]
-        return np.where(kind == SLIP_WALL, wall, np.where(kind == FIXED_STATE, self.fixed3, interior))
+        return np.where(kind == SLIP_WALL, wall, np.where(kind >= FIXED_STATE, self.fixed3, interior))
 
     def troubled_cell_limit(self, q, avg):
         """limiting.py:136-163. Returns (limited q, troubled flags (K,))."""

@@ -238,7 +238,10 @@ def test_adjoint_buffer_sizes():
     # + 2 positivity theta / node) doubles
     assert lib.cfd_tape_bytes(ld, _native.CFD_FP64) == 5 * 60 * ld * 8 + 27 * ld * 8
     assert lib.cfd_tape_bytes(ld, _native.CFD_FP32_MIXED) == 5 * 60 * ld * 4 + 27 * ld * 8
-    assert lib.cfd_adjoint_work_bytes(ld, _native.CFD_FP64) == 252 * ld * 8 + 4 * ld + 256
+    # adjoint scratch: 252 rows of reals, the replay list (ld ints), its counter slot, the listed
+    # flags (ld bytes rounded up to 256)
+    assert lib.cfd_adjoint_work_bytes(ld, _native.CFD_FP64) == 252 * ld * 8 + 4 * ld + 256 + 256
+    assert lib.cfd_adjoint_work_bytes(300, _native.CFD_FP32_MIXED) == 252 * 300 * 4 + 4 * 300 + 256 + 512
     assert lib.cfd_tape_bytes(0, _native.CFD_FP64) == -1
     assert lib.cfd_adjoint_work_bytes(ld, 9) == -1
 
