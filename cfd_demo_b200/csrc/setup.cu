@@ -264,6 +264,10 @@ __global__ void cs_kernel(const SetupArgs A) {
       const int tag = A.nb_f[3 * e + f];  // -1: untagged (reported in the status)
       const bool known = tag >= 0 && tag < A.in.num_tags;
       kind = known ? A.in.tag_kind[tag] : CFD_FACE_SLIP_WALL;
+      if (kind != CFD_FACE_SLIP_WALL && kind != CFD_FACE_FIXED_STATE) {
+        atomicOr(A.status, CFD_SETUP_UNSUPPORTED_KIND);
+        kind = CFD_FACE_SLIP_WALL;
+      }
       nbr = known && kind == CFD_FACE_FIXED_STATE ? A.in.tag_row[tag] : 0;
     }
     A.neighbor[f * ld + e] = nbr;

@@ -135,7 +135,8 @@ typedef struct CfdMeshBuild {
     const int64_t* elements;       /* [K][3] counterclockwise vertex ids, each < num_vertices */
     const int64_t* boundary_edges; /* [nb][2] vertex ids of every tagged boundary edge */
     const int32_t* boundary_tag;   /* [nb] tag index of each edge */
-    const int32_t* tag_kind;       /* [tags] CFD_FACE_SLIP_WALL | CFD_FACE_FIXED_STATE */
+    const int32_t* tag_kind;       /* [tags] CFD_FACE_SLIP_WALL | CFD_FACE_FIXED_STATE (exact-state
+                                      tags need per-node rows: build those tables on the host) */
     const int32_t* tag_row;        /* [tags] bc_states row of a fixed-state tag */
 } CfdMeshBuild;
 
@@ -147,6 +148,7 @@ typedef struct CfdMeshBuild {
 #define CFD_SETUP_NO_COEFFICIENTS 16      /* no nonnegative Cockburn-Shu coefficients */
 #define CFD_SETUP_NOT_CONFORMING_NODES 32 /* neighbouring face nodes do not coincide */
 #define CFD_SETUP_TABLE_FULL 64           /* internal hash table full (not expected) */
+#define CFD_SETUP_UNSUPPORTED_KIND 128    /* a tag of another kind than slip wall / fixed state */
 
 /* Per instance and per RK stage reduction slots (zeroed by cfd_rk3_attempt). */
 typedef struct CfdStageAcc {
