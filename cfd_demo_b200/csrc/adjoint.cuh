@@ -627,6 +627,24 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const AdjParams P) {
 // qt_bar tile is staged in shared memory. Node j's thread owns every output
 // at node j: the volume term at j and the surface terms of the face slots
 // that meet at j (corner nodes lie on two faces).
+// For each node j, the face slots (f * NFP + k) whose face node is j: none
+// (interior nodes), one, or two (the corners lie on two faces), packed as
+// slot + 1 in 6-bit fields.
+struct NodeSlotTable {
+  int v[NP];
+};
+constexpr NodeSlotTable make_node_slots() {
+  NodeSlotTable t{};
+  for (int j = 0; j < NP; ++j) {
+    int n = 0, packed = 0;
+    for (int sl = 0; sl < 3 * NFP; ++sl)
+      if ((int)((FN_PACK >> (4 * sl)) & 15ull) == j) packed |= (sl + 1) << (6 * n++);
+    t.v[j] = packed;
+  }
+  return t;
+}
+__device__ constexpr NodeSlotTable NODE_SLOTS = make_node_slots();
+
 constexpr int ADJ_EPB = 32;
 constexpr int ADJ_NODE_MINB = 1;  // resident blocks per SM the register budget is sized for
 
@@ -683,10 +701,12 @@ __global__ void __launch_bounds__(ADJ_EPB * NP, ADJ_NODE_MINB) adj_rhs_node_kern
   }
   // surface: the face slots (f, k) whose node is j
   const int finfo = m.face_info[e];
+  const int slots = NODE_SLOTS.v[j];  // warp-uniform
 #pragma unroll 1
-  for (int sl = 0; sl < 3 * NFP; ++sl) {
+  for (int u = 0; u < 2; ++u) {
+    const int sl = ((slots >> (6 * u)) & 63) - 1;
+    if (sl < 0) break;
     const int f = sl / NFP, k = sl - f * NFP;
-    if (face_node_rt(f, k) != j) continue;  // warp-uniform
     const int info = (finfo >> (8 * f)) & 0xff;
     const int kind = info & 3;
     const R nx = (R)m.face_geo[(3 * f) * ld + e], ny = (R)m.face_geo[(3 * f + 1) * ld + e];

@@ -329,9 +329,9 @@ static void launch_limit_two_pass(const LimitParams& p, int bs, cudaStream_t st)
   if (bs == 64) limit_scan_kernel<R, PHI, 64><<<g, 64, 0, st>>>(p);
   else if (bs == 256) limit_scan_kernel<R, PHI, 256><<<g, 256, 0, st>>>(p);
   else limit_scan_kernel<R, PHI, 128><<<g, 128, 0, st>>>(p);
-  // the list's length is only known on the device: enough threads for a
-  // quarter of the elements in one sweep (blocks beyond the list end exit at
-  // once; a longer list is swept grid-stride)
+  // the list's length is only known on the device: four threads per listed
+  // element, enough for a sixteenth of the elements in one sweep (blocks
+  // beyond the list end exit at once; a longer list is swept grid-stride)
   const unsigned full = blocks_for(p.m.num_elements, 64), cap = 32 * 148;
   limit_rewrite_kernel<R, PHI><<<full < cap ? full : cap, 64, 0, st>>>(p);
 }
