@@ -270,8 +270,8 @@ __device__ __forceinline__ void adj_limit_decide(const AdjParams& P, int e, doub
 }
 
 // Light pass over every element: where the limiters left the element as it
-// was, qt_bar = g and the neighbour-average adjoints are zero, which the
-// consumers read from g and from the listed flags instead of a copy; the
+// was, qt_bar = g and the neighbour-average adjoints are zero (adj_lift_kernel
+// reads g and the listed flags instead of a copy); the
 // others (troubled or positivity-scaled, a small minority) are flagged and
 // listed for adj_limit_heavy_kernel.
 template <typename R, int PHI>
@@ -289,22 +289,6 @@ __global__ void __launch_bounds__(128) adj_limit_scan_kernel(const AdjParams P) 
   }
   warp_list_append(P.list, P.count, listed, e);  // every lane of the warp takes part
   if (e < m.ld) P.listed[e] = listed ? 1 : 0;
-}
-
-// Whether element e's qt_bar lives in qtb (written by the heavy pass for a
-// listed element, or by adj_lift_kernel when a listed neighbour added the
-// adjoint of this element's average) rather than being g itself. Every
-// consumer evaluates the same predicate.
-__device__ __forceinline__ bool adj_uses_qtb(const AdjParams& P, int e) {
-  if (P.listed[e]) return true;
-  if (!P.limited) return false;
-  const CfdMesh& m = P.m;
-  const int finfo = m.face_info[e];
-  bool any = false;
-#pragma unroll
-  for (int f = 0; f < 3; ++f)
-    if (((finfo >> (8 * f)) & 3) == CFD_FACE_INTERIOR) any |= P.listed[m.neighbor[f * m.ld + e]] != 0;
-  return any;
 }
 
 // qt_bar = Lambda'(qt)^T g for one listed element, plus the adjoints of the
@@ -588,8 +572,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const AdjParams P) {
   for (int i = 0; i < NP; ++i) vi[i] = src[(c * NP + i) * ld + e];
   if (P.limited) {
     // the listed neighbours' adjoints of this element's average (they read
-    // it in their troubled-cell tests): qt_bar += AVG_W * sum, written to
-    // qtb for the node pass whenever a neighbour is listed (adj_uses_qtb)
+    // it in their troubled-cell tests): qt_bar += AVG_W * sum
     const int finfo = m.face_info[e];
     const R* __restrict__ nab = (const R*)P.nab;
     R ab = R(0);
@@ -605,12 +588,13 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const AdjParams P) {
     }
     if (nb_listed) {
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        vi[i] += (R)tab::AVG_W[i] * ab;
-        v[(c * NP + i) * ld + e] = vi[i];
-      }
+      for (int i = 0; i < NP; ++i) vi[i] += (R)tab::AVG_W[i] * ab;
     }
   }
+  // the node pass reads qt_bar from qtb for every element (the pass-through
+  // elements' g is copied here, where it is in registers anyway)
+#pragma unroll
+  for (int i = 0; i < NP; ++i) v[(c * NP + i) * ld + e] = vi[i];
 #pragma unroll
   for (int col = 0; col < 3 * NFP; ++col) {
     R t = R(0);
@@ -656,14 +640,22 @@ __global__ void __launch_bounds__(ADJ_EPB * NP, ADJ_NODE_MINB) adj_rhs_node_kern
   const int lane = threadIdx.x, j = threadIdx.y;
   const int e = blockIdx.x * ADJ_EPB + lane;
   const bool in = e < m.num_elements;
-  const R* __restrict__ vsrc = (const R*)(in && adj_uses_qtb(P, e) ? P.qtb : P.g);
+  const R* __restrict__ qtb = (const R*)P.qtb;
+  const R* __restrict__ qs = (const R*)P.qs;
+  // this node's state and the element's metric, loaded ahead of the staging
+  // barrier so that their latency overlaps it
+  R q[4];
 #pragma unroll
-  for (int r = j; r < 4 * NP; r += NP) s_v[r][lane] = in ? vsrc[r * ld + e] : R(0);
+  for (int c = 0; c < 4; ++c) q[c] = in ? qs[(c * NP + j) * ld + e] : R(1);
+  const R rx = in ? (R)m.metric[e] : R(0), ry = in ? (R)m.metric[ld + e] : R(0);
+  const R sx = in ? (R)m.metric[2 * ld + e] : R(0), sy = in ? (R)m.metric[3 * ld + e] : R(0);
+  const int finfo = in ? m.face_info[e] : 0;
+#pragma unroll
+  for (int r = j; r < 4 * NP; r += NP) s_v[r][lane] = in ? qtb[r * ld + e] : R(0);
   __syncthreads();
   if (!in) return;
   const int inst = element_instance(m, e);
   if (inst < 0) return;
-  const R* __restrict__ qs = (const R*)P.qs;
   const R* __restrict__ w = (const R*)P.w;
   R* __restrict__ sb = (R*)P.src_bar;
   R* __restrict__ bb = (R*)P.base_bar;
@@ -674,11 +666,8 @@ __global__ void __launch_bounds__(ADJ_EPB * NP, ADJ_NODE_MINB) adj_rhs_node_kern
     for (int c = 0; c < 4; ++c) bb[(c * NP + j) * ld + e] += (R)P.a * s_v[c * NP + j][lane];
   }
   // volume at node j: Ft_bar_j = -sum_i Dr[i][j] v_i, Gt_bar_j likewise
-  R q[4], acc[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) q[c] = qs[(c * NP + j) * ld + e];
+  R acc[4];
   {
-    const R rx = (R)m.metric[e], ry = (R)m.metric[ld + e], sx = (R)m.metric[2 * ld + e], sy = (R)m.metric[3 * ld + e];
     R fb[4], gb[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -700,7 +689,6 @@ __global__ void __launch_bounds__(ADJ_EPB * NP, ADJ_NODE_MINB) adj_rhs_node_kern
     for (int c = 0; c < 4; ++c) acc[c] = (R)P.b * s_v[c * NP + j][lane] + jf[c] + jg[c];
   }
   // surface: the face slots (f, k) whose node is j
-  const int finfo = m.face_info[e];
   const int slots = NODE_SLOTS.v[j];  // warp-uniform
 #pragma unroll 1
   for (int u = 0; u < 2; ++u) {
