@@ -108,7 +108,9 @@ __global__ void __launch_bounds__(2 * BatchShape<R>::EPB, BatchShape<R>::MINB)
   }
 }
 
-// Host side: one persistent launch of a precision and flux, every limiter.
+// Host side: one persistent launch of a precision and flux, every limiter:
+// as many blocks as are resident on the GPU, or as there are element tiles
+// if that is fewer.
 template <typename R, int FLUX, int PHI>
 cudaError_t launch_batch_phi(const BatchParams& b, cudaStream_t st) {
   // b.attempts == 0: only the per-device lookup below, no launch
@@ -134,8 +136,12 @@ cudaError_t launch_batch_phi(const BatchParams& b, cudaStream_t st) {
     grid_of[dev] = per_sm * sms;
   }
   if (b.attempts == 0) return cudaSuccess;
+  // no more blocks than element tiles: every phase strides over its work, and
+  // a grid barrier over fewer blocks is cheaper for a small batch
+  const int ntiles = (b.s.mesh.num_elements + SH::EPB - 1) / SH::EPB;
+  const int grid = ntiles < 1 ? 1 : (ntiles < grid_of[dev] ? ntiles : grid_of[dev]);
   void* args[] = {const_cast<BatchParams*>(&b)};
-  return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid_of[dev]), dim3(2 * SH::EPB), args, L::BYTES, st);
+  return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(2 * SH::EPB), args, L::BYTES, st);
 }
 
 template <typename R, int FLUX>

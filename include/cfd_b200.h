@@ -291,7 +291,8 @@ int cfd_run_control(const CfdSolver* s, void* stream);
  * for every instance in ONE persistent, cooperative launch (no counterpart in
  * the reference, which solves one problem per EulerSolver; this is the
  * batched form of its run loop, solver.py:180-204). The grid holds as many
- * blocks as are resident on the GPU at once; they loop over the element
+ * blocks as are resident on the GPU at once (or one per element tile of 64
+ * elements, if there are fewer tiles); they loop over the element
  * tiles of all instances, with a grid-wide barrier between the phases of an
  * attempt (zero the reduction slots; stage k and its limiter passes for
  * k = 1, 2, 3; report and control). Returns early once no instance is active.
