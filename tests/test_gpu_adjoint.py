@@ -204,6 +204,53 @@ def test_smooth_state_random_direction_unlimited(flux, report):
     assert _rel(ad_bc, central_bc) < 1e-6
 
 
+@pytest.mark.parametrize("flux", ["rusanov", "hllc"])
+def test_exact_state_boundaries_random_direction_unlimited(flux, report):
+    """Exact-state faces (one exterior row per face node) on two sides of the
+    smooth case: the gradient in the initial state and in the per-node
+    exterior rows against central differences."""
+    from cfd_demo_b200 import EulerSolver, ExactState, FixedState, SolverConfig
+    from cfd_demo_b200.adjoint import AdjointRun, cfl_schedule, differentiable_run
+
+    base, q, x, y = _smooth_case(flux, seed=2)
+
+    def far(xx, yy):
+        rho = 1.0 + 0.2 * np.sin(2.0 * xx + 1.0) * np.cos(3.0 * yy)
+        u, v, p = 0.1 + 0.05 * np.cos(xx), -0.05 + 0.03 * np.sin(yy), 1.0 + 0.1 * np.sin(xx + yy)
+        return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=-1)
+
+    mean = FixedState.from_primitive(1.0, 0.1, -0.05, 1.0, 1.4)
+    bcs = {"left": mean, "bottom": mean, "top": ExactState(far), "right": ExactState(far)}
+    solver = EulerSolver(base.mesh, bcs, SolverConfig(flux=flux, limiter="unlimited", gamma=1.4))
+    dts = cfl_schedule(solver, q, steps=12)
+    runner = AdjointRun(solver, dts, checkpoint_every=5)
+    dev = solver.operators.device
+    weight = torch.from_numpy(np.exp(-((x - 0.8) ** 2 + (y - 0.8) ** 2) / 0.05)).to(dev)
+    rng = np.random.default_rng(11)
+    direction = torch.from_numpy(rng.normal(size=q.shape)).to(dev)
+    cotangent = torch.from_numpy(rng.normal(size=4)).to(dev)
+
+    def objective(qf):
+        return ((qf * cotangent).sum(-1) * weight).sum()
+
+    q0 = torch.from_numpy(q).to(dev).requires_grad_(True)
+    bc = solver.operators.bc_states.clone().requires_grad_(True)
+    assert bc.shape[0] == 1 + 6 * (12 + 10)  # one fixed row, six rows per exact-state face
+    j = objective(differentiable_run(runner, q0, bc))
+    j.backward()
+    adjoint = float((q0.grad * direction).sum())
+    with torch.no_grad():
+        central, _ = _quotients(lambda s: differentiable_run(runner, q0 + s * direction, bc), objective)
+    dbc = torch.from_numpy(rng.normal(size=bc.shape)).to(dev)
+    ad_bc = float((bc.grad * dbc).sum())
+    with torch.no_grad():
+        central_bc, _ = _quotients(lambda s: differentiable_run(runner, q0, bc + s * dbc), objective)
+    report(f"adjoint smooth 12x10 {flux}/unlimited 12 steps, exact-state top and right: state rel "
+           f"{_rel(adjoint, central):.1e}, exterior rows rel {_rel(ad_bc, central_bc):.1e}")
+    assert _rel(adjoint, central) < 1e-6
+    assert _rel(ad_bc, central_bc) < 1e-6
+
+
 def test_checkpoint_interval_does_not_change_the_gradient():
     from cfd_demo_b200.adjoint import AdjointRun
 
