@@ -14,7 +14,10 @@ resident, loop over the tiles of every instance and step through the phases
 of each attempt with grid-wide barriers; the chunk's launch is captured in a
 CUDA graph and replayed. ``persistent=False``: CUDA-graph chunks of the
 separate launches (cfd_rk3_attempt + cfd_run_control per attempt). Either
-way the host polls the loop states once per chunk.
+way the host polls the loop states once per chunk. Once the instances still
+running hold at most half of the batch's elements, `run` / `run_to` repack
+them into a smaller batch (same tables, states and loop states), so that the
+launches stop sweeping the tiles of finished instances.
 
 `riemann_batch` builds the seeded benchmark family: Riemann problems on
 [0,1]x[0,0.1] strips split at x = 0.5 with left/right density and pressure
@@ -71,7 +74,7 @@ class BatchedEulerSolver:
     """Several independent problems with one configuration, advanced together."""
 
     def __init__(self, cases, config: SolverConfig, *, device="cuda", graph_chunk: int = 64, variant: int = 0,
-                 persistent: bool = True):
+                 persistent: bool = True, compact: bool = True, _parts=None):
         import torch
 
         if not torch.cuda.is_available():
@@ -79,13 +82,19 @@ class BatchedEulerSolver:
         self.config = config
         self.reference = build_reference_triangle(DEGREE)
         self.cases = list(cases)
-        parts = []
-        for case in self.cases:
-            conn = build_connectivity(case.mesh)
-            geo = element_geometry(case.mesh)
-            kind, state = resolve_boundary_conditions(conn, case.boundary_conditions)
-            parts.append(host_tables(case.mesh, conn, geo, self.reference, kind, state, device=device,
-                                     boundary_conditions=case.boundary_conditions))
+        if _parts is None:
+            parts = []
+            for case in self.cases:
+                conn = build_connectivity(case.mesh)
+                geo = element_geometry(case.mesh)
+                kind, state = resolve_boundary_conditions(conn, case.boundary_conditions)
+                parts.append(host_tables(case.mesh, conn, geo, self.reference, kind, state, device=device,
+                                         boundary_conditions=case.boundary_conditions))
+        else:
+            parts = list(_parts)
+        self._parts = parts
+        self._device = device
+        self.compact = bool(compact)
         self.precision = PRECISIONS[config.precision]
         self.operators = DeviceTables(parts, device, self.precision)
         self._ws = Workspace(self.operators, self.precision, config.limiter != "unlimited")
@@ -134,14 +143,59 @@ class BatchedEulerSolver:
         stopped by a bad CFL step or too many rejections, without raising),
         or `max_attempts` attempts have run (instances still active are left
         so); returns the loop states (CfdControl) of all instances."""
+        where = self._march(states, final_time, max_chunk or self._graph_chunk, max_attempts, True)
+        return [c for _, _, c in where]
+
+    def _march(self, states, final_time, cap_chunk: int, max_attempts, graph: bool) -> list:
+        """Begin a run and advance in chunks of attempts (1, 2, 4, ... up to
+        cap_chunk) until no instance is active or max_attempts attempts have
+        run. With `compact`, whenever the active instances hold at most half
+        of the current batch's elements they are repacked into a smaller
+        batch (`_subset`), so that the launches stop sweeping the tiles of
+        finished instances. Returns per instance (batch holding its final
+        state, its index there, its loop state)."""
         self.begin_run(states, final_time)
-        chunk, cap, done = 1, max_chunk or self._graph_chunk, 0
+        cur, ids = self, list(range(self.num_instances))
+        where: list = [None] * self.num_instances
+        chunk, done = 1, 0
         while True:
-            ctl = self.advance(chunk)
+            ctl = cur.advance(chunk, graph=graph)
             done += chunk
-            if all(c.status != _native.RUN_ACTIVE for c in ctl) or (max_attempts and done >= max_attempts):
-                return ctl
-            chunk = min(2 * chunk, cap)
+            for k, i in enumerate(ids):
+                where[i] = (cur, k, ctl[k])
+            active = [k for k, c in enumerate(ctl) if c.status == _native.RUN_ACTIVE]
+            if not active or (max_attempts and done >= max_attempts):
+                return where
+            if cur.compact and len(active) < len(ctl):
+                live = sum(int(cur.operators.sizes[k]) for k in active)
+                if 2 * live <= cur.num_elements:
+                    cur, ids = cur._subset(active, ctl), [ids[k] for k in active]
+            chunk = min(2 * chunk, cap_chunk)
+
+    def _subset(self, keep: list, ctl: list) -> "BatchedEulerSolver":
+        """A batch of the instances `keep` (indices into this batch) that
+        carries on from their current states and loop states (read at a chunk
+        boundary). The tables are this batch's host tables (not rebuilt); each
+        state is copied into the new batch's first buffer and its loop state's
+        parity set to match. Tiles never straddle instances, so every element
+        is computed exactly as it would have been in this batch."""
+        import torch
+
+        sub = BatchedEulerSolver([self.cases[i] for i in keep], self.config, device=self._device,
+                                 graph_chunk=self._graph_chunk, variant=self._struct.variant,
+                                 persistent=self.persistent, compact=self.compact,
+                                 _parts=[self._parts[i] for i in keep])
+        sub._struct.block_size = self._struct.block_size
+        raw = bytearray()
+        for k, i in enumerate(keep):
+            c = _native.CfdControl.from_buffer_copy(bytes(ctl[i]))
+            src = self._ws.x1 if c.parity else self._ws.x0
+            o, n, on = int(self.operators.offsets[i]), int(self.operators.sizes[i]), int(sub.operators.offsets[k])
+            sub._ws.x0[:, on:on + n].copy_(src[:, o:o + n])
+            c.parity = 0
+            raw += bytes(c)
+        sub._ws.control.copy_(torch.frombuffer(raw, dtype=torch.uint8).to(sub._ws.control.device))
+        return sub
 
     def set_block_size(self, block: int) -> None:
         self._struct.block_size = int(block)
@@ -245,13 +299,8 @@ class BatchedEulerSolver:
         per instance (same fields as EulerSolver.run)."""
         start = time.perf_counter()
         states = [c.initial_state for c in self.cases] if states is None else states
-        self.begin_run(states, final_time)
-        chunk = 1
-        while True:
-            ctl = self.advance(chunk, graph=graph)
-            if all(c.status != _native.RUN_ACTIVE for c in ctl):
-                break
-            chunk = min(2 * chunk, self._graph_chunk)
+        where = self._march(states, final_time, self._graph_chunk, None, graph)
+        ctl = [c for _, _, c in where]
         failed = [(i, c) for i, c in enumerate(ctl) if c.status not in (_native.RUN_DONE,)]
         if failed:
             i, c = failed[0]
@@ -259,9 +308,9 @@ class BatchedEulerSolver:
             raise SolverError(f"Instance {i} stopped at t = {c.time}: {what} ({len(failed)} instance(s) failed).")
         wall = time.perf_counter() - start
         out = []
-        for i, c in enumerate(ctl):
-            x = self._ws.x1 if c.parity else self._ws.x0
-            out.append(RunResult(state=self.download(x, i), time=float(c.time), steps=int(c.steps),
+        for b, k, c in where:
+            x = b._ws.x1 if c.parity else b._ws.x0
+            out.append(RunResult(state=b.download(x, k), time=float(c.time), steps=int(c.steps),
                                  rejected_steps=int(c.rejected), boundary_flux_integral=np.array(c.flux_integral[:]),
                                  min_density=float(c.min_density), min_pressure=float(c.min_pressure),
                                  max_troubled_cells=int(c.max_troubled), wall_time=wall))

@@ -47,6 +47,33 @@ def test_batch_instances_finish_at_their_own_times(persistent):
         assert np.all(np.isfinite(r.state))
 
 
+@pytest.mark.parametrize("persistent", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
+def test_repacking_finished_instances_changes_no_result(precision, persistent):
+    """Instances with staggered final times: the run that repacks the still
+    active instances into smaller batches as the others finish gives every
+    instance the same steps, times and states, bit for bit, as the run that
+    keeps sweeping the full batch."""
+    from cfd_demo_b200 import SolverConfig
+    from cfd_demo_b200.batch import BatchedEulerSolver, riemann_batch
+
+    cases = riemann_batch(count=10, seed=5, nx_range=(10, 50))
+    cfg = SolverConfig(flux="hllc", limiter="superbee", gamma=1.4, precision=precision)
+    times = np.linspace(0.002, 0.03, len(cases))[::-1].copy()
+    packed = BatchedEulerSolver(cases, cfg, persistent=persistent, compact=True)
+    full = BatchedEulerSolver(cases, cfg, persistent=persistent, compact=False)
+    a, b = packed.run(final_time=times), full.run(final_time=times)
+    for x, y in zip(a, b):
+        assert (x.steps, x.rejected_steps, x.max_troubled_cells) == (y.steps, y.rejected_steps, y.max_troubled_cells)
+        assert x.time == y.time
+        assert np.array_equal(x.state, y.state)
+        assert x.min_density == y.min_density and x.min_pressure == y.min_pressure
+        np.testing.assert_allclose(x.boundary_flux_integral, y.boundary_flux_integral, rtol=1e-12, atol=1e-15)
+    # the packed run did repack: instance 0 (the latest final time) finished in a smaller batch
+    where = packed._march([c.initial_state for c in cases], times, 64, None, True)
+    assert where[0][0] is not packed and where[0][0].num_instances < len(cases)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
 @pytest.mark.parametrize("flux,limiter", [("rusanov", "minmod"), ("roe", "unlimited"), ("hllc", "van_leer"),
                                           ("hllc", "superbee"), ("rusanov", "mc")])
