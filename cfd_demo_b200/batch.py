@@ -14,10 +14,13 @@ resident, loop over the tiles of every instance and step through the phases
 of each attempt with grid-wide barriers; the chunk's launch is captured in a
 CUDA graph and replayed. ``persistent=False``: CUDA-graph chunks of the
 separate launches (cfd_rk3_attempt + cfd_run_control per attempt). Either
-way the host polls the loop states once per chunk. Once the instances still
-running hold at most half of the batch's elements, `run` / `run_to` repack
-them into a smaller batch (same tables, states and loop states), so that the
-launches stop sweeping the tiles of finished instances.
+way the host polls the loop states once per chunk. With ``compact=True``,
+once the instances still running hold at most half of the batch's elements,
+`run` / `run_to` repack them into a smaller batch (same tables, states and
+loop states), so that the launches stop sweeping the tiles of finished
+instances. Off by default: the blocks of finished instances exit at once, so
+on the seeded family repacking bought nothing against its table uploads and
+graph captures.
 
 `riemann_batch` builds the seeded benchmark family: Riemann problems on
 [0,1]x[0,0.1] strips split at x = 0.5 with left/right density and pressure
@@ -74,7 +77,7 @@ class BatchedEulerSolver:
     """Several independent problems with one configuration, advanced together."""
 
     def __init__(self, cases, config: SolverConfig, *, device="cuda", graph_chunk: int = 64, variant: int = 0,
-                 persistent: bool = True, compact: bool = True, _parts=None):
+                 persistent: bool = True, compact: bool = False, _parts=None):
         import torch
 
         if not torch.cuda.is_available():
