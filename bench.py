@@ -704,6 +704,77 @@ def run_precision(args) -> dict:
     }
 
 
+def _oblique_oracle_rate(nx: int, ny: int, steps: int) -> float:
+    """The oracle's DOF-steps/s on the oblique-shock case (one process)."""
+    import oracle
+    from oracle.physics import ExactState as OExact, FixedState as OFixed, SlipWall as OSlip
+
+    from cfd_demo_b200.cases import OBLIQUE_GAMMA, OBLIQUE_HEIGHT, OBLIQUE_LENGTH
+    from cfd_demo_b200.mesh import sheared_rectangle_mesh
+    from cfd_demo_b200.verification import ObliqueShock
+
+    ex = ObliqueShock(2.0, math.radians(10.0), OBLIQUE_GAMMA)
+    m = sheared_rectangle_mesh(nx, ny, ex.theta, (0.0, OBLIQUE_LENGTH), (0.0, OBLIQUE_HEIGHT))
+    om = oracle.mesh.TriangleMesh(np.array(m.vertices), np.array(m.elements),
+                                  {k: np.array(v) for k, v in m.boundary_edges.items()})
+    far = OExact(ex.conserved, ex.cell_average)
+    s = oracle.OracleSolver(om, {"left": OFixed.from_primitive(*ex.upstream, OBLIQUE_GAMMA), "bottom": OSlip(),
+                                 "top": far, "right": far}, flux="rusanov", limiter="minmod", gamma=OBLIQUE_GAMMA)
+    q = np.broadcast_to(np.array(OFixed.from_primitive(*ex.upstream, OBLIQUE_GAMMA).state), s.state_shape).copy()
+    q, _ = s.step(q, s.time_step(q))  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        q, _ = s.step(q, s.time_step(q))
+    return steps * m.num_elements * NP_NODES / (time.perf_counter() - t0)
+
+
+def run_oblique(args) -> dict:
+    """The oblique-shock verification case (exact far-field boundaries on a
+    sheared mesh; CFD-demo proposes it in its ADR 0011 / 0012): baseline
+    M1 = 2, wall 10 deg, rusanov/minmod, FP64, 200x100 quads x 2 (K = 40,000)
+    to t = 2 through EulerSolver.run, timed on the wall clock; the ADR's
+    acceptance quantities; the oracle's rate on the same mesh (a few steps,
+    one host core) beside it."""
+    import torch
+
+    from cfd_demo_b200 import oblique_shock
+    from cfd_demo_b200.verification import oblique_l1_errors, shock_angle_at
+
+    nx, ny = args.oblique_nx, args.oblique_nx // 2
+    oracle_rate = _oblique_oracle_rate(nx, ny, 3) if not args.no_cpu_baseline else None
+    torch.cuda.set_device(0)
+    case = oblique_shock(nx, ny, flux="rusanov", limiter="minmod")
+    s, ex = case.solver, case.exact
+    from cfd_demo_b200.autotune import autotune
+
+    shape = autotune(s, case.initial_state)["choice"] if args.variant is None else (args.variant, 0)
+    if args.variant is not None:
+        s.set_variant(args.variant)
+    s.run(case.initial_state, 0.01)  # warm-up: captures the run loop's graphs
+    initial = s.integrate(case.initial_state)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = s.run(case.initial_state, case.final_time)
+    wall = time.perf_counter() - t0
+    q = torch.from_numpy(res.state).cuda()
+    err = oblique_l1_errors(q, s.mesh, ex, 1.4)
+    angle = shock_angle_at(q, s.mesh, ex, 0.5 * case.length, case.height)
+    defect = s.integrate(res.state) - initial + res.boundary_flux_integral
+    rate = res.steps * s.mesh.num_elements * NP_NODES / wall
+    return {
+        "metric": "oblique-shock run DOF-steps/s (EulerSolver.run, wall clock)", "value": rate,
+        "unit": "DOF-steps/s", "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"oblique shock M1 = 2, wall 10 deg, {nx}x{ny} quads x 2 (K={s.mesh.num_elements}), "
+                               "rusanov/minmod, exact far-field top and right, t = 0 -> 2"},
+        "stage_kernel": list(shape), "steps": res.steps, "seconds": wall,
+        "l1": {k: v for k, v in err.items() if k != "area"},
+        "shock_angle_deg": math.degrees(angle), "exact_beta_deg": math.degrees(ex.beta),
+        "conservation_defect_max": float(np.abs(defect).max()),
+        "cpu_oracle": {"value": oracle_rate, "unit": "DOF-steps/s", "cores": 1, "kind": "port",
+                       "sample": f"3 RK3 steps of the same {nx}x{ny} case after one warm-up step"},
+    }
+
+
 def run_reference(args) -> dict:
     """The reference arm: the CPU oracle (NumPy restatement of the reference's
     own algorithm; the reference itself is JAX code that cannot be installed
@@ -741,7 +812,9 @@ def main() -> None:
                     help="stage-kernel variant of the FP64 form (default: as --variant); fixing both to the "
                          "autotuner's choices reproduces a run's kernels under a profiler, whose serialised "
                          "launches would mislead the autotuner")
-    ap.add_argument("--workload", choices=["microbenchmark", "batch", "adjoint", "precision"], default="microbenchmark")
+    ap.add_argument("--workload", choices=["microbenchmark", "batch", "adjoint", "precision", "oblique"],
+                    default="microbenchmark")
+    ap.add_argument("--oblique-nx", type=int, default=200)
     ap.add_argument("--precision-nx", type=int, default=2000)
     ap.add_argument("--precision-quad", type=int, default=6)
     ap.add_argument("--adjoint-steps", type=int, default=200)
@@ -775,6 +848,10 @@ def main() -> None:
     if args.workload == "precision":
         if rank == 0:
             print(json.dumps(run_precision(args)), flush=True)
+        return
+    if args.workload == "oblique":
+        if rank == 0:
+            print(json.dumps(run_oblique(args)), flush=True)
         return
 
     if args.impl == "reference":
