@@ -1,6 +1,6 @@
 """Autotuner of the stage-kernel shape (elements per block, tile staging).
 
-The fused stage kernel comes in ten shapes (CfdSolver.variant):
+The fused stage kernel comes in these shapes (CfdSolver.variant):
   0  tiled, 32 elements (64 threads) per block, state and geometry staged in
      shared memory, stage base read from global memory in the epilogue
   1  tiled, 32 elements per block, stage base staged in shared memory too
@@ -24,6 +24,11 @@ The fused stage kernel comes in ten shapes (CfdSolver.variant):
      evaluates each face flux once for both sides and lifts the 15 jump
      inputs of each element from shared memory
   11 shape 8 (staged base rows) in the face-job form
+  12, 13  shape 9 with the volume node loop kept rolled ([Dr|Ds] columns from
+     the constant bank: a fifteenth of the unrolled loop's code, every entry
+     taken), with unrolled / rolled face rounds
+  14 shape 5 with the volume node loop kept rolled
+  (6, 7 and 12-14 are not among the default candidates)
 `autotune(solver, state)` times one RK3 attempt per candidate on the solver's
 own buffers (an attempt from the same state recomputes the same step, so the
 candidates see identical work), keeps the fastest, and remembers the choice per
@@ -37,6 +42,9 @@ import math
 
 from . import _native
 
+# shapes 12-14 are selectable but not candidates: measured on the 1M-element
+# workload they lose in FP32 (12: 1.497, 13: 1.465 ms against 1.284 ms for 9)
+# and tie in FP64 (14: 2.941 ms against 2.963 ms for 5)
 CANDIDATES = ((0, 0), (1, 0), (3, 0), (4, 0), (5, 0), (8, 0), (9, 0), (10, 0), (11, 0), (2, 64), (2, 128))  # (variant, pair-kernel block size)
 _cache: dict = {}
 

@@ -460,7 +460,7 @@ void launch_stage_flux(const StageParams& p, int flux, int bs, cudaStream_t st) 
   else launch_stage_bs<R, 2, MODE>(p, bs, st);
 }
 template <typename R, int FLUX, int MODE, int EPB, bool SB, int MINB = (sizeof(R) == 4 ? 512 : 384) / (2 * EPB),
-          bool UF = true, bool PK = true, bool CF = false, bool FJ = false>
+          bool UF = true, bool PK = true, bool CF = false, bool FJ = false, bool VR = false>
 void launch_tile(const StageParams& p, cudaStream_t st) {
   using L = TileLayout<R, EPB, SB, FJ>;
   constexpr bool PACK = PK && sizeof(R) == 4;  // FP64 shares the unpacked instantiation
@@ -473,12 +473,12 @@ void launch_tile(const StageParams& p, cudaStream_t st) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= MAX_DEV || !configured[dev]) {
-    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL, FJ>,
+    cudaFuncSetAttribute(stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL, FJ, VR>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
     if (dev >= 0 && dev < MAX_DEV) configured[dev] = true;
   }
   const unsigned g = blocks_for(p.m.num_elements, EPB);
-  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL, FJ><<<g, 2 * EPB, L::BYTES, st>>>(p);
+  stage_tile_kernel<R, FLUX, MODE, EPB, SB, MINB, UF, PACK, CALL, FJ, VR><<<g, 2 * EPB, L::BYTES, st>>>(p);
 }
 template <typename R, int FLUX, int MODE>
 void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_t st) {
@@ -496,6 +496,14 @@ void launch_stage_variant(const StageParams& p, int variant, int bs, cudaStream_
   else if (variant == 10)
     launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, true, true, true, true>(p, st);
   else if (variant == 11) launch_tile<R, FLUX, MODE, 64, true, sizeof(R) == 4 ? 3 : 2, true, true, true, true>(p, st);
+  // 12 / 13: variant 9 with the volume node loop kept rolled, with unrolled / rolled face rounds;
+  // 14: variant 5 with the volume node loop kept rolled (smaller code)
+  else if (variant == 12)
+    launch_tile<R, FLUX, MODE, 64, true, (sizeof(R) == 4 ? 512 : 384) / 128, true, true, true, false, true>(p, st);
+  else if (variant == 13)
+    launch_tile<R, FLUX, MODE, 64, true, (sizeof(R) == 4 ? 512 : 384) / 128, false, true, true, false, true>(p, st);
+  else if (variant == 14)
+    launch_tile<R, FLUX, MODE, 64, false, (sizeof(R) == 4 ? 512 : 384) / 128, false, true, false, false, true>(p, st);
   else launch_tile<R, FLUX, MODE, 32, false>(p, st);
 }
 // One precision and mode of the stage kernels, every flux and shape; each

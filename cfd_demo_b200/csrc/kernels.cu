@@ -285,7 +285,7 @@ static int validate(const CfdSolver* s) {
   if (!(s->gamma > 1.0)) return fail(CFD_E_ARG, "gamma must be greater than one");
   if (s->block_size != 0 && s->block_size != 64 && s->block_size != 128 && s->block_size != 256)
     return fail(CFD_E_ARG, "block_size must be 0, 64, 128 or 256");
-  if (s->variant < 0 || s->variant > 11) return fail(CFD_E_ARG, "variant must be 0..11");
+  if (s->variant < 0 || s->variant > 14) return fail(CFD_E_ARG, "variant must be 0..14");
   if (s->variant != 2 && s->mesh.instance && s->mesh.num_instances > 1 && (s->mesh.flags & 1) == 0)
     return fail(CFD_E_ARG, "tiled stage kernels need instance ranges aligned to 64 elements (CfdMesh.flags bit 0)");
   return CFD_OK;

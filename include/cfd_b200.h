@@ -216,7 +216,10 @@ typedef struct CfdSolver {
                               8 tiled with 64 elements per block + staged base rows,
                               9 as 8 with the face-node flux as an out-of-line call (FP32),
                               10 / 11 the face-job form of 3 / 8: each face's flux is evaluated
-                              once, by the block's owner of the face, for both of its sides */
+                              once, by the block's owner of the face, for both of its sides,
+                              12 / 13 as 9 with the volume node loop kept rolled ([Dr|Ds] from
+                              the constant bank), with unrolled / rolled face rounds,
+                              14 as 5 with the volume node loop kept rolled */
     int32_t* limit_list;   /* optional [CFD_LIMIT_LIST_HEADER + ld] scratch: with it the limiter
                               runs in two passes (a light detection pass over every element,
                               then the rewrite of the troubled / non-positive ones only);

@@ -93,7 +93,7 @@ def test_positivity_floor_is_met_exactly():
 
 @pytest.mark.parametrize("flux", FLUXES)
 @pytest.mark.parametrize("limiter", LIMITERS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14])
 def test_step_matches_reference(flux, limiter, variant):
     g = load("step")
     s = make_solver(g, "mesh", flux=flux, limiter=limiter, variant=variant)
@@ -140,7 +140,7 @@ def test_short_sod_stage_troubled_counts_match_per_step():
         assert rep.admissible
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14])
 def test_fp32_mixed_step_tracks_fp64(variant):
     """The FP32-mixed form against the plain form on the step fixture: one RK3
     step agrees to FP32 accuracy (1e-5 of each variable's scale)."""
