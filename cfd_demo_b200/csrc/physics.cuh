@@ -154,9 +154,11 @@ __device__ __forceinline__ void roe(const R qm[4], const R qp[4], const Prim<R>&
   const R dun = (wp.u * nx + wp.v * ny) - (wm.u * nx + wm.v * ny);
   const R dut = (-wp.u * ny + wp.v * nx) - (-wm.u * ny + wm.v * nx);
   const R c2 = c * c;
-  const R i2c2 = rcp(R(2) * c2);
+  const R ic2 = rcp(c2);
+  const R i2c2 = R(0.5) * ic2;  // = rcp(2 c2): exact in FP64 (a power-of-two scaling commutes with
+                                 // the correctly rounded reciprocal), one reciprocal fewer per flux
   const R a_m = (dp - rho * c * dun) * i2c2;
-  const R a_e = drho - dp * rcp(c2);
+  const R a_e = drho - dp * ic2;
   const R a_s = rho * dut;
   const R a_p = (dp + rho * c * dun) * i2c2;
   const R delta = R(0.1) * (abs_(un) + c);
