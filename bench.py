@@ -62,12 +62,12 @@ FALLBACK_HBM_GBS = 6650.0
 # scaled to a launch of the benchmark by its element count (traffic grows in
 # proportion to K). Writes still in L2 when a launch ends are not counted
 # there, so the stage result's 240 / 480 B appear partly.
-NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (480.7, 739.9, 750.1), "fp64": (1008.8, 1523.9, 1527.1)}
+NCU_BYTES_PER_ELEMENT = {"fp32_mixed": (480.2, 739.5, 750.5), "fp64": (1007.3, 1522.3, 1528.0)}
 # Warp instructions issued per element of each stage launch (ncu
 # smsp__inst_executed.sum / K, same captures). With 148 SMs issuing at most
 # 4 warp instructions per cycle each, they bound a launch from below at
 # instructions / (148 * 4 * SM clock): the instruction-issue roofline.
-NCU_WARP_INSTRUCTIONS_PER_ELEMENT = {"fp32_mixed": (267.1, 289.7, 305.5), "fp64": (518.1, 533.1, 587.3)}
+NCU_WARP_INSTRUCTIONS_PER_ELEMENT = {"fp32_mixed": (267.0, 289.2, 304.9), "fp64": (512.1, 527.1, 581.3)}
 SMS, ISSUE_PER_SM_CYCLE = 148, 4
 
 
