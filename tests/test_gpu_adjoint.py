@@ -328,7 +328,7 @@ def _smooth_bump_direction(case, seed):
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_sod_400x40_random_smooth_direction(seed, report):
-    """Config 3 (Sod 400x40, 200 steps, checkpoints every 20): <dJ/dq0, d>
+    """The sensitivity study (Sod 400x40, 200 steps, checkpoints every 20): <dJ/dq0, d>
     for random smooth density directions d in the bump region. The adjoint
     must agree with the fourth-order difference quotient (h = 1e-4) to 1e-4
     relative, and with the central quotient (eps = 1e-6) within that
