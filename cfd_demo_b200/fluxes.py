@@ -25,7 +25,8 @@ def _device_flux(flux_id: int) -> Callable:
         shape = np.broadcast_shapes(qm.shape[:-1], qp.shape[:-1], np.shape(nx), np.shape(ny))
         arrs = [np.broadcast_to(qm, shape + (4,)), np.broadcast_to(qp, shape + (4,)),
                 np.broadcast_to(np.asarray(nx, np.float64), shape), np.broadcast_to(np.asarray(ny, np.float64), shape)]
-        dev = [torch.as_tensor(np.ascontiguousarray(a)).reshape(-1).cuda() for a in arrs]
+        # copies: broadcast views are read-only, which torch does not accept as tensor storage
+        dev = [torch.from_numpy(np.array(a, dtype=np.float64)).reshape(-1).cuda() for a in arrs]
         n = int(np.prod(shape)) if shape else 1
         out = torch.empty(4 * n, dtype=torch.float64, device="cuda")
         lib = _native.load()

@@ -21,7 +21,7 @@ def _device_phi(limiter_id: int) -> Callable:
         from . import _native
 
         ra = np.asarray(r, dtype=np.float64)
-        d = torch.as_tensor(np.ascontiguousarray(ra)).reshape(-1).cuda()
+        d = torch.from_numpy(np.array(ra, dtype=np.float64)).reshape(-1).cuda()  # a copy: r may be read-only
         out = torch.empty_like(d)
         _native.check(_native.load().cfd_limiter_phi(limiter_id, d.numel(), d.data_ptr(), out.data_ptr(),
                                                      torch.cuda.current_stream().cuda_stream))
